@@ -1,0 +1,255 @@
+"""Seeded synthetic initial fields for the DIM step.
+
+Each generator returns ``(desc, soa)``: a descriptor (include/dimgpu.h) and a
+C-contiguous FP64 SoA field of shape (V, ncell), x-fastest.  Identical arrays
+are fed to the GPU path and to the CPU checkers, so no initial-condition code
+path can differ between them.
+
+Shapes follow the reference's own validation precedents (Riemann tubes,
+shock-bubble, bubble clouds); all values are drawn from ``numpy`` generators
+seeded per call.  Diffuse interfaces use the reference's tanh indicator
+``0.5 * (1 - tanh(a * s / thickness))`` (src/setup/dim_initial_conditions.hpp:
+224-236) with thickness = 2 cells and a = 2.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass
+
+import numpy as np
+
+from .abi import Desc, make_desc
+
+ALPHA_FLOOR = 1e-6
+
+
+def prim_to_cons_np(dim: int, mats, alpha: np.ndarray, rho: np.ndarray,
+                    vel: np.ndarray, p: np.ndarray) -> np.ndarray:
+    """Vectorised primitive -> conservative map of one field.
+
+    alpha, rho: (nmat, n); vel: (dim, n); p: (n,).  Same formulas as
+    dim::prim_to_cons (src/dim/primitives.hpp:165-212) for ideal and
+    stiffened gas; used only to build initial fields.
+    """
+    nmat = len(mats)
+    n = p.shape[0]
+    out = np.empty((2 * nmat + dim, n))
+    m = alpha * rho
+    rho_t = np.maximum(m.sum(axis=0), 1e-12)
+    rho_e = np.zeros(n)
+    for k, (kind, gamma, p_inf) in enumerate(mats):
+        e_k = (p + gamma * p_inf) / ((gamma - 1.0) * rho[k])
+        rho_e += alpha[k] * rho[k] * e_k
+    ke = 0.5 * rho_t * (vel * vel).sum(axis=0)
+    out[:nmat] = m
+    out[nmat:nmat + dim] = rho_t * vel
+    out[nmat + dim] = rho_e + ke
+    out[nmat + dim + 1:] = alpha[:nmat - 1]
+    return out
+
+
+def smooth_indicator(signed_distance, thickness, sharpness=2.0):
+    """Reference tanh indicator, 1 inside (s <= 0), 0 outside."""
+    return 0.5 * (1.0 - np.tanh(max(sharpness, 1e-12) * signed_distance / thickness))
+
+
+def _kind(p_inf: float) -> str:
+    return "stiffened_gas" if p_inf > 0.0 else "ideal_gas"
+
+
+@dataclass
+class SideState:
+    gamma: float
+    p_inf: float
+    rho: float
+    p: float
+    u: float
+
+
+def draw_side(rng: np.random.Generator) -> SideState:
+    """One side of the two-material Riemann problem (config-0 distributions)."""
+    gamma = rng.uniform(1.4, 6.1)
+    p_inf = 0.0 if rng.uniform() < 0.5 else rng.uniform(1e8, 6e8)
+    rho = math.exp(rng.uniform(math.log(0.1), math.log(1000.0)))
+    p = math.exp(rng.uniform(math.log(1e4), math.log(1e9)))
+    u = rng.uniform(-100.0, 100.0)
+    return SideState(gamma, p_inf, rho, p, u)
+
+
+def riemann(seed: int = 0, N=(1000,), axis: int = 0, position: float = 0.5,
+            lengths=None, bc=None) -> tuple[Desc, np.ndarray]:
+    """Two-material Riemann problem (config 0 in 1D; any axis in 2D/3D).
+
+    Left cells hold material 0 with alpha = 1 - 1e-6 and material 1 at
+    alpha = 1e-6 (its own side's density); right cells the reverse.
+    """
+    rng = np.random.default_rng(seed)
+    L, R = draw_side(rng), draw_side(rng)
+    dim = len(N)
+    lengths = lengths or [1.0] * dim
+    dx = [lengths[a] / N[a] for a in range(dim)]
+    mats = [(_kind(L.p_inf), L.gamma, L.p_inf), (_kind(R.p_inf), R.gamma, R.p_inf)]
+    desc = make_desc(dim, N, dx, mats, bc_lo=bc, bc_hi=bc)
+    coords = np.meshgrid(*[(np.arange(N[a]) + 0.5) * dx[a] for a in reversed(range(dim))],
+                         indexing="ij")
+    x = coords[dim - 1 - axis].reshape(-1)
+    left = x < position * lengths[axis]
+    n = x.size
+    alpha = np.empty((2, n))
+    alpha[0] = np.where(left, 1.0 - ALPHA_FLOOR, ALPHA_FLOOR)
+    alpha[1] = 1.0 - alpha[0]
+    rho = np.empty((2, n))
+    rho[0] = L.rho
+    rho[1] = R.rho
+    vel = np.zeros((dim, n))
+    vel[axis] = np.where(left, L.u, R.u)
+    p = np.where(left, L.p, R.p)
+    soa = prim_to_cons_np(dim, mats, alpha, rho, vel, p)
+    return desc, np.ascontiguousarray(soa)
+
+
+def rankine_hugoniot(mach: float, gamma: float, rho1: float, p1: float):
+    """Post-shock (rho, u, p) of a shock of Mach `mach` running into rest."""
+    m2 = mach * mach
+    p2 = p1 * (1.0 + 2.0 * gamma / (gamma + 1.0) * (m2 - 1.0))
+    rho2 = rho1 * (gamma + 1.0) * m2 / ((gamma - 1.0) * m2 + 2.0)
+    c1 = math.sqrt(gamma * p1 / rho1)
+    u2 = mach * c1 * (1.0 - rho1 / rho2)
+    return rho2, u2, p2
+
+
+def shock_bubble_2d(N=(1024, 512), seed: int = 0) -> tuple[Desc, np.ndarray]:
+    """Config 1: Mach 1.22 shock at x = 0.6 hitting a light bubble.
+
+    Domain [0,2]x[0,1]; ambient gamma 1.4, rho 1, p 1; bubble gamma 1.67,
+    rho 0.138, radius 0.25 at (1, 0.5); post-shock slab x < 0.6 moving +x.
+    Transmissive in x, reflective in y.  (The seed is unused: the case is
+    deterministic.)
+    """
+    nx, ny = N
+    dx = [2.0 / nx, 1.0 / ny]
+    mats = [("ideal_gas", 1.4, 0.0), ("ideal_gas", 1.67, 0.0)]
+    desc = make_desc(2, N, dx, mats, bc_lo=["transmissive", "reflective"],
+                     bc_hi=["transmissive", "reflective"])
+    rho2, u2, p2 = rankine_hugoniot(1.22, 1.4, 1.0, 1.0)
+    y, x = np.meshgrid((np.arange(ny) + 0.5) * dx[1], (np.arange(nx) + 0.5) * dx[0], indexing="ij")
+    x = x.reshape(-1)
+    y = y.reshape(-1)
+    sd = np.hypot(x - 1.0, y - 0.5) - 0.25
+    thick = 2.0 * max(dx)
+    ab = smooth_indicator(sd, thick)
+    ab = np.where(ab <= 1e-14, 0.0, ab)
+    post = x < 0.6
+    rho_amb = np.where(post, rho2, 1.0)
+    p_amb = np.where(post, p2, 1.0)
+    u_amb = np.where(post, u2, 0.0)
+    n = x.size
+    alpha = np.stack([1.0 - ab, ab])
+    rho = np.stack([rho_amb, np.full(n, 0.138)])
+    vel = np.stack([(1.0 - ab) * u_amb, np.zeros(n)])
+    p = (1.0 - ab) * p_amb + ab * 1.0
+    soa = prim_to_cons_np(2, mats, alpha, rho, vel, p)
+    return desc, np.ascontiguousarray(soa)
+
+
+def bubble_cloud_3d(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64,
+                    pulse_width: float = 0.05) -> tuple[Desc, np.ndarray]:
+    """Config 2: 64 seeded air bubbles in water, 1e9 Pa slab at x < 0.05.
+
+    Water: stiffened gas gamma 4.4, p_inf 6e8, rho 1000, p 1e5.  Air: ideal
+    gamma 1.4, rho 1.2, p 1e5.  Radii U[0.02, 0.06], rejection-sampled to be
+    non-overlapping (with one cell of clearance).  Transmissive everywhere.
+    """
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = N
+    dx = [1.0 / nx, 1.0 / ny, 1.0 / nz]
+    mats = [("stiffened_gas", 4.4, 6e8), ("ideal_gas", 1.4, 0.0)]
+    desc = make_desc(3, N, dx, mats)
+    bubbles = []
+    tries = 0
+    while len(bubbles) < nbubbles and tries < 100000:
+        tries += 1
+        r = rng.uniform(0.02, 0.06)
+        c = rng.uniform(r + pulse_width, 1.0 - r, size=3)
+        c[1:] = rng.uniform(r, 1.0 - r, size=2)
+        if all(np.linalg.norm(c - b[0]) > r + b[1] + 2 * max(dx) for b in bubbles):
+            bubbles.append((c, r))
+    thick = 2.0 * max(dx)
+    ncell = nx * ny * nz
+    air = np.zeros(ncell)
+    air3 = air.reshape(nz, ny, nx)
+    reach = 6.0 * thick
+    for c, r in bubbles:
+        lo = [max(0, int((c[a] - r - reach) / dx[a])) for a in range(3)]
+        hi = [min(N[a], int((c[a] + r + reach) / dx[a]) + 1) for a in range(3)]
+        zs = (np.arange(lo[2], hi[2]) + 0.5) * dx[2]
+        ys = (np.arange(lo[1], hi[1]) + 0.5) * dx[1]
+        xs = (np.arange(lo[0], hi[0]) + 0.5) * dx[0]
+        Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
+        sd = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r
+        ind = smooth_indicator(sd, thick)
+        sub = air3[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
+        np.maximum(sub, ind, out=sub)
+    air[air <= 1e-14] = 0.0
+    out = np.empty((2 * 2 + 3, ncell))
+    chunk = nx * ny * 16
+    xs_all = (np.arange(nx) + 0.5) * dx[0]
+    for s in range(0, ncell, chunk):
+        e = min(ncell, s + chunk)
+        a1 = air[s:e]
+        n = e - s
+        x = np.tile(xs_all, n // nx)
+        p = np.where(x < pulse_width, 1e9, 1e5)
+        alpha = np.stack([1.0 - a1, a1])
+        rho = np.stack([np.full(n, 1000.0), np.full(n, 1.2)])
+        vel = np.zeros((3, n))
+        out[:, s:e] = prim_to_cons_np(3, mats, alpha, rho, vel, p)
+    return desc, out
+
+
+def single_bubble_2d(N, seed: int = 0) -> tuple[Desc, np.ndarray]:
+    """A config-0 material pair with one circular bubble of the second one."""
+    rng = np.random.default_rng(seed)
+    A, B = draw_side(rng), draw_side(rng)
+    nx, ny = N
+    dx = [1.0 / nx, 1.0 / ny]
+    mats = [(_kind(A.p_inf), A.gamma, A.p_inf), (_kind(B.p_inf), B.gamma, B.p_inf)]
+    desc = make_desc(2, N, dx, mats)
+    cx, cy = rng.uniform(0.3, 0.7, size=2)
+    r = rng.uniform(0.1, 0.25)
+    y, x = np.meshgrid((np.arange(ny) + 0.5) * dx[1], (np.arange(nx) + 0.5) * dx[0], indexing="ij")
+    sd = (np.hypot(x - cx, y - cy) - r).reshape(-1)
+    ab = smooth_indicator(sd, 2.0 * max(dx))
+    ab = np.clip(ab, ALPHA_FLOOR, 1.0 - ALPHA_FLOOR)
+    n = sd.size
+    alpha = np.stack([1.0 - ab, ab])
+    rho = np.stack([np.full(n, A.rho), np.full(n, B.rho)])
+    vel = np.zeros((2, n))
+    vel[0] = (1.0 - ab) * A.u + ab * B.u
+    p = (1.0 - ab) * A.p + ab * B.p
+    soa = prim_to_cons_np(2, mats, alpha, rho, vel, p)
+    return desc, np.ascontiguousarray(soa)
+
+
+def random_states(desc: Desc, n: int, seed: int = 0, edge_fraction: float = 0.1) -> np.ndarray:
+    """Record-major random conservative states, including edge cases
+    (near-zero and zero fractions, tiny or negative masses, large momenta)."""
+    rng = np.random.default_rng(seed)
+    nmat, dim = desc.nmat, desc.dim
+    mats = [(desc.mat[k].kind, desc.mat[k].gamma, desc.mat[k].p_inf) for k in range(nmat)]
+    alpha = rng.dirichlet(np.ones(nmat), size=n).T
+    rho = np.exp(rng.uniform(np.log(0.1), np.log(1000.0), size=(nmat, n)))
+    p = np.exp(rng.uniform(np.log(1e-2), np.log(1e9), size=n))
+    vel = rng.uniform(-300.0, 300.0, size=(dim, n))
+    U = prim_to_cons_np(dim, mats, alpha, rho, vel, p).T.copy()
+    ne = int(edge_fraction * n)
+    if ne:
+        idx = rng.choice(n, size=ne, replace=False)
+        q = len(idx) // 5
+        if nmat > 1:
+            U[idx[:q], nmat + dim + 1] = 0.0                      # alpha_0 = 0
+            U[idx[q:2 * q], nmat + dim + 1] = 1e-11               # alpha below inactive floor
+        U[idx[2 * q:3 * q], 0] *= -1e-3                                # negative mass
+        U[idx[3 * q:4 * q], nmat + dim] *= 1e-6                        # energy deficit
+        U[idx[4 * q:], nmat:nmat + dim] *= 50.0                        # large momentum
+    return U

@@ -1,0 +1,196 @@
+/*
+ * dimgpu.h — C-ABI of the B200-native Allaire five-equation diffuse-interface
+ * (DIM) time step.
+ *
+ * The library replaces the header-only, OpenMP-parallel DIM step of
+ * SegunOwoeye/diffuse_vs_GFM_MMS.  Every entry point below names the reference
+ * function it stands in for (paths relative to the reference project root).
+ * Signatures are plain C: pointers, sizes and POD structs only, so the
+ * reference's C++ host (or ctypes, or any FFI) can bind them directly.
+ *
+ * State layout (host and device): structure of arrays, FP64, component-major.
+ * Component c of cell `linear` lives at soa[c * ncell + linear], where the
+ * linear index is x-fastest exactly as in the reference
+ * (src/dim/solver/advance/geometry.hpp:26-53).  The components of one cell are
+ * the fields of dim::State<DIM> (src/dim/state.hpp:9-15) in declaration order:
+ *
+ *     partial_mass[0 .. nmat-1], mom[0 .. DIM-1], E, alpha[0 .. nmat-2]
+ *
+ * so V = 2*nmat + DIM components per cell (V = 5, 6, 7 for two materials in
+ * 1D, 2D, 3D).
+ *
+ * Status codes: every call returns DIMGPU_OK (0) or a positive error code;
+ * dimgpu_last_error() gives a one-line message.  The reference throws
+ * std::runtime_error in the same situations; the C++ drop-in header
+ * (dimgpu_reference_shim.hpp) turns a non-zero status back into that throw.
+ *
+ * Threading: a session is not thread-safe; distinct sessions may be used from
+ * distinct host threads.  All device work of a session is ordered on the
+ * session's CUDA stream.
+ */
+#ifndef DIMGPU_H
+#define DIMGPU_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DIMGPU_MAX_MATERIALS 4
+
+/* Status codes. */
+enum {
+    DIMGPU_OK = 0,
+    DIMGPU_E_INVALID_ARG = 1,     /* bad sizes, dt_max <= 0, cfl <= 0, gamma <= 1, ... */
+    DIMGPU_E_UNSUPPORTED_EOS = 2, /* an EoS kind other than ideal / stiffened gas      */
+    DIMGPU_E_NONFINITE = 3,       /* a non-finite or non-positive time step             */
+    DIMGPU_E_TIMEOUT = 4,         /* a bounded device-side wait ran out                 */
+    DIMGPU_E_OOM = 5,             /* device allocation failed / admission refused       */
+    DIMGPU_E_CUDA = 6,            /* any other CUDA runtime error                       */
+    DIMGPU_E_UNSUPPORTED = 7      /* valid option that this build does not implement    */
+};
+
+/* EoS kinds: same numbering as the reference's EOSKind
+ * (src/euler/eos_params.hpp:8-15).  Only the first two run on the GPU. */
+enum {
+    DIMGPU_EOS_IDEAL_GAS = 0,
+    DIMGPU_EOS_STIFFENED_GAS = 1,
+    DIMGPU_EOS_NOBLE_ABEL = 2,
+    DIMGPU_EOS_PENG_ROBINSON = 3,
+    DIMGPU_EOS_TAIT = 4,
+    DIMGPU_EOS_MIE_GRUNEISEN = 5
+};
+
+/* Boundary kinds (Config::bc_lo / bc_hi strings, src/io/config.hpp:131-132).
+ * Any name other than "reflective" / "nonreflective" behaves as transmissive
+ * in the reference (src/dim/solver/advance/boundary.hpp:201-224). */
+enum {
+    DIMGPU_BC_TRANSMISSIVE = 0,
+    DIMGPU_BC_REFLECTIVE = 1,
+    DIMGPU_BC_NONREFLECTIVE = 2
+};
+
+/* Config::dim_lambda_model (src/io/config.hpp:124). */
+enum {
+    DIMGPU_LAMBDA_KAPILA = 0,
+    DIMGPU_LAMBDA_ALLAIRE = 1,
+    DIMGPU_LAMBDA_EQUAL_VELOCITY = 2
+};
+
+/* Arithmetic of the step. */
+enum {
+    DIMGPU_PRECISION_FP64 = 0,  /* bit-faithful to the reference's double run        */
+    DIMGPU_PRECISION_MIXED = 1  /* FP32 reconstruction + HLLC, FP64 state/EoS/dt      */
+};
+
+/* Config::time_update (src/io/config.hpp:112). */
+enum {
+    DIMGPU_TIME_SPLIT = 0,
+    DIMGPU_TIME_UNSPLIT = 1
+};
+
+/* One material: the fields of ::EOSParams that the ideal and stiffened-gas
+ * laws read (src/euler/eos_params.hpp:46-53). */
+typedef struct dimgpu_material {
+    int kind;
+    double gamma;
+    double p_inf;
+} dimgpu_material;
+
+/* Everything the reference's step reads from N, dx, dim::EOSParams and
+ * Config<DIM> (src/dim/solver/advance_step.hpp:150-158). */
+typedef struct dimgpu_desc {
+    int dim;                        /* 1, 2 or 3                                  */
+    int N[3];                       /* cells per axis; unused axes must be 1      */
+    double dx[3];                   /* spacing per axis                           */
+    int nmat;                       /* 1 .. DIMGPU_MAX_MATERIALS                  */
+    dimgpu_material mat[DIMGPU_MAX_MATERIALS];
+    int bc_lo[3];                   /* DIMGPU_BC_* per axis                       */
+    int bc_hi[3];
+    int lambda_model;               /* DIMGPU_LAMBDA_*                            */
+    double alpha_source_floor;      /* Config::dim_alpha_source_floor             */
+    int precision;                  /* DIMGPU_PRECISION_*                         */
+    int time_update;                /* DIMGPU_TIME_*                              */
+} dimgpu_desc;
+
+/* Per-call phase timings, the device-side counterpart of SolverPhaseTimings
+ * (src/core/phase_timings.hpp:4-12).  Milliseconds, from CUDA events. */
+typedef struct dimgpu_phase_times {
+    double cfl_ms;
+    double sweep_ms;
+    double boundary_ms;
+} dimgpu_phase_times;
+
+typedef struct dimgpu_session dimgpu_session;
+
+/* Number of doubles per cell for a descriptor (2*nmat + dim). */
+int dimgpu_components(const dimgpu_desc* desc);
+
+/* Create a session: validates the descriptor (dim::EOSParams::validate,
+ * src/dim/eos_params.hpp:16-28) and allocates the device-resident SoA state.
+ * Unsupported EoS kinds give DIMGPU_E_UNSUPPORTED_EOS; there is no CPU path. */
+int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out);
+
+/* Free a session and all its device memory. */
+int dimgpu_destroy(dimgpu_session* s);
+
+/* Message of the last failing call on this session (or of the last failing
+ * session-less call when s is NULL).  Never NULL. */
+const char* dimgpu_last_error(const dimgpu_session* s);
+
+/* Copy `count` doubles (must be V * ncell) from a host SoA buffer into the
+ * session.  Replaces the caller's std::vector<dim::State<DIM>> argument of
+ * dim::advance_one_step (src/dim/solver/advance_step.hpp:150-151). */
+int dimgpu_upload(dimgpu_session* s, const double* soa, size_t count);
+
+/* Copy the session state into a host SoA buffer of `count` doubles.
+ * Replaces StepResult::U_new (src/dim/solver/advance_step.hpp:141-146). */
+int dimgpu_download(dimgpu_session* s, double* soa, size_t count);
+
+/* One full time step on the resident state: CFL dt, then the split x, y, z
+ * sweeps, each followed by the boundary fill.  Replaces
+ * dim::advance_one_step (src/dim/solver/advance_step.hpp:150-270).
+ * dt_out receives the step's dt; times may be NULL. */
+int dimgpu_step(dimgpu_session* s, double cfl, double dt_max, double* dt_out,
+                dimgpu_phase_times* times);
+
+/* n consecutive steps with the same cfl and dt_max, no host synchronisation
+ * between them (the CFL minimum of step k+1 is fused into step k's last
+ * sweep).  dt_out (may be NULL) receives n doubles.  Equivalent to n calls of
+ * dimgpu_step, i.e. to the time loop of run_dim_case with a constant dt_max
+ * (src/app/solver/run_dim.hpp:88-111). */
+int dimgpu_steps(dimgpu_session* s, int n, double cfl, double dt_max, double* dt_out);
+
+/* CFL time step of the resident state.  Replaces dim::compute_dt_cfl
+ * (src/dim/solver/cfl.hpp:16-66) and, for DIMGPU_TIME_UNSPLIT sessions,
+ * dim::compute_dt_cfl_unsplit (src/dim/solver/cfl.hpp:70-119). */
+int dimgpu_compute_dt_cfl(dimgpu_session* s, double cfl, double dt_max, double* dt_out);
+
+/* One split sweep along `dir` with time step dt, in place on the resident
+ * state.  Replaces dim::sweep_direction_dispatch
+ * (src/dim/solver/advance/sweep_core.hpp:151-202). */
+int dimgpu_sweep_direction(dimgpu_session* s, int dir, double dt);
+
+/* Boundary fill of the resident state.  Replaces
+ * dim::apply_boundary_conditions (src/dim/solver/advance/boundary.hpp:165-226). */
+int dimgpu_apply_boundary_conditions(dimgpu_session* s);
+
+/* Mass per material, momentum per axis and total energy summed over all
+ * cells and multiplied by the cell volume; out receives nmat + dim + 1
+ * doubles.  Device counterpart of compute_dim_conservation_totals
+ * (src/app/io/conservation_report.hpp:188-218). */
+int dimgpu_totals(dimgpu_session* s, double* out);
+
+/* Stateless drop-in for one call of dim::advance_one_step
+ * (src/dim/solver/advance_step.hpp:150-270): host SoA in, host SoA out.
+ * Uses a cached session per descriptor shape; the copies are part of the call. */
+int dimgpu_advance_one_step(const dimgpu_desc* desc, const double* soa_in, double* soa_out,
+                            double cfl, double dt_max, double* dt_out,
+                            dimgpu_phase_times* times);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DIMGPU_H */
