@@ -1,0 +1,185 @@
+// dim_line.h — the split sweep of one line (dim::solve_line,
+// src/dim/solver/advance/sweep_core.hpp:16-149, with
+// reconstruct_line_interfaces, src/dim/reconstruction/muscl.hpp:197-329)
+// factored into five per-cell stages whose only coupling is to the nearest
+// neighbour of the previous stage:
+//
+//   A  cell i:  P_i = cons_to_prim(U_i)                    (one bisection)
+//   B  cell i:  needs Pe_{i-1}, Pe_{i+1} -> U_half_i, Ph_i  (one bisection)
+//   C  cell i:  needs Ph_{i-1}, Ph_{i+1} -> face states LS_i, RS_i and their
+//               primitives PLS_i, PRS_i                     (two bisections)
+//   D  face i|i+1: needs RS_i, PRS_i, LS_{i+1}, PLS_{i+1} -> HLLC flux F,
+//               face velocity s*, upwind alpha flux
+//   E  cell i:  needs the faces i-1|i and i|i+1 -> U_out_i
+//
+// The CUDA kernel runs the stages over a shared-memory tile with one
+// __syncthreads between them; tests/native runs them over a host array.  The
+// reference computes the same quantities line-wide; the factorisation
+// removes its duplicate recoveries without changing any value:
+//  * primitive[i] and P_line[i] share one cons_to_prim (P_line = enforce(P));
+//  * P_half of an end cell is P_line of that cell (U_half = U there);
+//  * the face primitives PL_face / PR_face are the cons_to_prim calls inside
+//    hllc_flux_normal (same states), computed once per face state;
+//  * the material sound speeds of alpha_rhs_coefficients depend on (rho_k, p)
+//    only, which P and enforce(P) share.
+#pragma once
+
+#include "dim_physics.h"
+
+namespace dimgpu {
+
+template<int NM, int D>
+struct CellA {
+    Prim<NM, D> P;   // cons_to_prim(U): un-enforced (primitive[i] in solve_line)
+    Prim<NM, D> Pe;  // enforce_positive_primitive(P)  (P_line[i])
+    double ck[NM];   // material sound speeds for alpha_rhs_coefficients
+};
+
+// Stage A.
+template<int NM, int D>
+DHD void stage_a(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
+{
+    cons_to_prim<NM, D>(M, U, A.P);
+    A.Pe = A.P;
+    enforce_positive_primitive<NM, D>(A.Pe);
+    rhs_sound_speeds<NM, D>(M, A.P, A.ck);
+}
+
+// Stage B.  `end` is true for the first and last cell of the line and for
+// every cell of a line shorter than 3 (no reconstruction there,
+// muscl.hpp:213-226, 244-252, 271-272).
+template<int NM, int D>
+DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
+                 const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, State<NM, D>& Uh,
+                 Prim<NM, D>& Ph)
+{
+    if (end) {
+        Uh = U;
+        Ph = A.Pe;
+        return;
+    }
+    Prim<NM, D> Pl, Pr;
+    reconstruct_cell_faces<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
+    State<NM, D> Ul, Ur;
+    prim_to_cons<NM, D>(M, Pl, Ul);
+    prim_to_cons<NM, D>(M, Pr, Ur);
+    repair_state<NM, D>(M, Ul);
+    repair_state<NM, D>(M, Ur);
+    hancock_predict<NM, D>(M, U, A.Pe, A.ck, Ul, Ur, Pl, Pr, dir, dt, dx, Uh);
+    cons_to_prim<NM, D>(M, Uh, Ph);
+    enforce_positive_primitive<NM, D>(Ph);
+}
+
+// Stage C: the half-step face states of cell i (U_left_half[i],
+// U_right_half[i]) and their primitives (the cons_to_prim of PL_face /
+// PR_face and of hllc_flux_normal).
+template<int NM, int D>
+DHD void stage_c(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Ph,
+                 const Prim<NM, D>& Ph_lo, const Prim<NM, D>& Ph_hi, bool end, State<NM, D>& LS,
+                 State<NM, D>& RS, Prim<NM, D>& PLS, Prim<NM, D>& PRS)
+{
+    if (end) {
+        LS = U;
+        RS = U;
+        PLS = A.P;
+        PRS = A.P;
+        return;
+    }
+    Prim<NM, D> Lh, Rh;
+    reconstruct_cell_faces<NM, D>(Ph_lo, Ph, Ph_hi, Lh, Rh);
+    prim_to_cons<NM, D>(M, Lh, LS);
+    prim_to_cons<NM, D>(M, Rh, RS);
+    repair_state<NM, D>(M, LS);
+    repair_state<NM, D>(M, RS);
+    cons_to_prim<NM, D>(M, LS, PLS);
+    cons_to_prim<NM, D>(M, RS, PRS);
+}
+
+// Stage D output per face.
+template<int NM, int D>
+struct FaceD {
+    Flux<NM, D> F;
+    double fv;       // face velocity s*
+    double af[NM];   // upwind alpha flux (sweep_core.hpp:119-127)
+};
+
+// Stage D: face between cell i (UL = RS_i) and cell i+1 (UR = LS_{i+1}).
+template<int NM, int D>
+DHD bool stage_d(const Mats& M, const State<NM, D>& UL, const Prim<NM, D>& PL, const State<NM, D>& UR,
+                 const Prim<NM, D>& PR, int dir, FaceD<NM, D>& out)
+{
+    const bool ok = hllc_flux<NM, D>(M, UL, UR, PL, PR, dir, out.F, out.fv);
+    const double* up = (out.fv >= 0.0) ? PL.alpha : PR.alpha;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) out.af[k] = up[k] * out.fv;
+    return ok;
+}
+
+// Stage E: conservative update + repair, then the non-conservative alpha
+// update + repair (sweep_core.hpp:96-148).  lo / hi are the faces i-1|i and
+// i|i+1; first / last mark the line's end cells, whose outer face copies the
+// inner one (F[0] = F[1], F[n] = F[n-1]) and whose outer alpha flux is the
+// cell-centred fraction times that face velocity.
+template<int NM, int D>
+DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const FaceD<NM, D>* lo,
+                 const FaceD<NM, D>* hi, bool first, bool last, double dt, double dx, State<NM, D>& out)
+{
+    const FaceD<NM, D>& Flo = first ? *hi : *lo;
+    const FaceD<NM, D>& Fhi = last ? *lo : *hi;
+    const double lambda = dt / dx;
+    out = U;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) out.m[k] -= lambda * (Fhi.F.m[k] - Flo.F.m[k]);
+#pragma unroll
+    for (int d = 0; d < D; ++d) out.mom[d] -= lambda * (Fhi.F.mom[d] - Flo.F.mom[d]);
+    out.E -= lambda * (Fhi.F.E - Flo.F.E);
+    repair_state<NM, D>(M, out);
+
+    double af_lo[NM], af_hi[NM];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        af_lo[k] = first ? A.P.alpha[k] * Flo.fv : Flo.af[k];
+        af_hi[k] = last ? A.P.alpha[k] * Fhi.fv : Fhi.af[k];
+    }
+    double rhs[NM];
+    alpha_rhs_coefficients<NM, D>(M, A.P, A.ck, rhs);
+    const double div_u = (Fhi.fv - Flo.fv) / dx;
+    double alpha_new[NM];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        alpha_new[k] = A.P.alpha[k];
+        alpha_new[k] -= lambda * (af_hi[k] - af_lo[k]);
+        alpha_new[k] += dt * rhs[k] * div_u;
+    }
+    sanitise_alpha<NM>(alpha_new, 0.0);
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) out.a[k] = alpha_new[k];
+    repair_state<NM, D>(M, out);
+}
+
+// CFL candidate of one cell (dim::compute_dt_cfl body, src/dim/solver/cfl.hpp:
+// 46-62, and the unsplit variant :94-115): the smallest cfl*dx_d/wave_speed
+// over the axes (or cfl/spectral_sum); +inf when no axis contributes.
+// P = cons_to_prim(U).
+template<int NM, int D>
+DHD double cfl_candidate(const Mats& M, const State<NM, D>& U, const Prim<NM, D>& P, const double* dx,
+                         double cfl, bool unsplit)
+{
+    const double c = generic_mixture_sound_speed<NM>(M, total_density<NM, D>(U), P.p, P.alpha, P.rho);
+    double best = HUGE_VAL;
+    if (unsplit) {
+        double spectral_sum = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d) spectral_sum += (fabs(P.vel[d]) + c) / dx[d];
+        if (spectral_sum > 1e-14) best = cfl / spectral_sum;
+        return best;
+    }
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        const double wave_speed = fabs(P.vel[d]) + c;
+        if (wave_speed > 1e-14) best = dmin(best, cfl * dx[d] / wave_speed);
+    }
+    return best;
+}
+
+}  // namespace dimgpu
