@@ -1,0 +1,642 @@
+// dim_kernels.cuh — CUDA kernels of the DIM step for sm_100a.
+//
+// State: FP64 structure of arrays in HBM, component c of cell i at
+// state[c * ncell + i], x-fastest.  One sweep kernel launch advances every
+// line along one axis by the split MUSCL-Hancock / HLLC update; the CFL
+// kernel reduces the step; the boundary kernel refills the boundary shell.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dim_launch.h"
+#include "dim_line.h"
+#include "dimgpu.h"
+
+namespace dimgpu {
+
+// ---- SoA load / store ----------------------------------------------------------
+template<int NM, int D>
+__device__ __forceinline__ void load_cell(const double* __restrict__ s, long long ncell, long long i,
+                                          State<NM, D>& U)
+{
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) U.m[k] = __ldg(s + (q++) * ncell + i);
+#pragma unroll
+    for (int d = 0; d < D; ++d) U.mom[d] = __ldg(s + (q++) * ncell + i);
+    U.E = __ldg(s + (q++) * ncell + i);
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) U.a[k] = __ldg(s + (q++) * ncell + i);
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void store_cell(double* __restrict__ s, long long ncell, long long i,
+                                           const State<NM, D>& U)
+{
+    int q = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) s[(q++) * ncell + i] = U.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) s[(q++) * ncell + i] = U.mom[d];
+    s[(q++) * ncell + i] = U.E;
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) s[(q++) * ncell + i] = U.a[k];
+}
+
+// ---- shared-memory records: variable v of slot t at sm[v * NT + t] -------------
+template<int NM, int D>
+__device__ __forceinline__ void sm_put(double* sm, int NT, int t, int v0, const Prim<NM, D>& P)
+{
+    int v = v0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sm[(v++) * NT + t] = P.rho[k];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sm[(v++) * NT + t] = P.alpha[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) sm[(v++) * NT + t] = P.vel[d];
+    sm[v * NT + t] = P.p;
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void sm_get(const double* sm, int NT, int t, int v0, Prim<NM, D>& P)
+{
+    int v = v0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) P.rho[k] = sm[(v++) * NT + t];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) P.alpha[k] = sm[(v++) * NT + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) P.vel[d] = sm[(v++) * NT + t];
+    P.p = sm[v * NT + t];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void sm_put(double* sm, int NT, int t, int v0, const State<NM, D>& U)
+{
+    int v = v0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sm[(v++) * NT + t] = U.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) sm[(v++) * NT + t] = U.mom[d];
+    sm[(v++) * NT + t] = U.E;
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) sm[(v++) * NT + t] = U.a[k];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void sm_get(const double* sm, int NT, int t, int v0, State<NM, D>& U)
+{
+    int v = v0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) U.m[k] = sm[(v++) * NT + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) U.mom[d] = sm[(v++) * NT + t];
+    U.E = sm[(v++) * NT + t];
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) U.a[k] = sm[(v++) * NT + t];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void sm_put(double* sm, int NT, int t, const FaceD<NM, D>& f)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sm[(v++) * NT + t] = f.F.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) sm[(v++) * NT + t] = f.F.mom[d];
+    sm[(v++) * NT + t] = f.F.E;
+    sm[(v++) * NT + t] = f.fv;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) sm[(v++) * NT + t] = f.af[k];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void sm_get(const double* sm, int NT, int t, FaceD<NM, D>& f)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) f.F.m[k] = sm[(v++) * NT + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) f.F.mom[d] = sm[(v++) * NT + t];
+    f.F.E = sm[(v++) * NT + t];
+    f.fv = sm[(v++) * NT + t];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) f.af[k] = sm[(v++) * NT + t];
+}
+
+__host__ __device__ constexpr int kPrimVars(int nm, int d) { return 2 * nm + d + 1; }
+__host__ __device__ constexpr int kStateVars(int nm, int d) { return 2 * nm + d; }
+// Largest live set between two stages: LS + PLS (stage C -> D).
+__host__ __device__ constexpr int kSweepSmemVars(int nm, int d) { return kStateVars(nm, d) + kPrimVars(nm, d); }
+
+// ---- the sweep kernel ------------------------------------------------------------
+//
+// CTA = T*W threads over W lines x T consecutive cells of each line.  For the
+// x sweep the T cells of a line are consecutive threads (coalesced); for the
+// y / z sweeps the W lines are W consecutive x columns and sit in consecutive
+// threads (coalesced across lines).  Cell positions pos = 0..T-1 map to line
+// cells tile*(T-6) - 3 + pos; positions 3..T-4 are written, the rest is halo.
+// Stage k+1 of a cell reads stage-k results of its two neighbours from shared
+// memory, so every stage is separated by one __syncthreads.
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
+                                                    Grid g, Mats M, int T, int W, int ntile, int ngx,
+                                                    const double* __restrict__ dtp, int* __restrict__ err)
+{
+    extern __shared__ double sm[];
+    const int NT = T * W;
+    const int t = threadIdx.x;
+    const int n = g.N[DIR];
+    const int OUT = T - 6;
+
+    int pos, j, s;
+    if (DIR == 0) { pos = t % T; j = t / T; s = 1; }
+    else { j = t % W; pos = t / W; s = W; }
+
+    // line of this thread and its base address
+    long long bid = blockIdx.x;
+    int tile;
+    long long base;
+    bool line_ok;
+    long long sline;
+    if (DIR == 0) {
+        tile = (int)(bid % ntile);
+        const long long L = (bid / ntile) * W + j;
+        const long long nlines = g.ncell / g.N[0];
+        line_ok = L < nlines;
+        base = L * g.N[0];
+        sline = 1;
+    }
+    else {
+        const int gx = (int)(bid % ngx);
+        const long long rest = bid / ngx;
+        tile = (int)(rest % ntile);
+        const long long other = rest / ntile;
+        const int x = gx * W + j;
+        line_ok = x < g.N[0];
+        if (DIR == 1) base = x + other * g.stride[2];
+        else base = x + other * g.stride[1];
+        sline = g.stride[DIR];
+    }
+    const int gi = tile * OUT - 3 + pos;
+    const bool valid = line_ok && gi >= 0 && gi < n;
+    const bool first = gi == 0, last = gi == n - 1;
+    const bool end = first || last || n < 3;
+    const long long cell = base + (long long)gi * sline;
+
+    const double dt = *dtp;
+    const double dx = g.dx[DIR];
+
+    // ---- stage A
+    State<NM, D> U;
+    CellA<NM, D> A;
+    if (valid) {
+        load_cell<NM, D>(in, g.ncell, cell, U);
+        stage_a<NM, D>(M, U, A);
+        sm_put<NM, D>(sm, NT, t, 0, A.Pe);
+    }
+    __syncthreads();
+
+    // ---- stage B
+    const bool needB = valid && (end || (pos >= 1 && pos <= T - 2));
+    State<NM, D> Uh;
+    Prim<NM, D> Ph;
+    if (needB) {
+        Prim<NM, D> lo, hi;
+        if (!end) {
+            sm_get<NM, D>(sm, NT, t - s, 0, lo);
+            sm_get<NM, D>(sm, NT, t + s, 0, hi);
+        }
+        stage_b<NM, D>(M, U, A, lo, hi, end, DIR, dt, dx, Uh, Ph);
+    }
+    __syncthreads();
+    if (needB) sm_put<NM, D>(sm, NT, t, 0, Ph);
+    __syncthreads();
+
+    // ---- stage C
+    auto needC_at = [&](int p, int gidx) {
+        const bool v = line_ok && gidx >= 0 && gidx < n;
+        const bool e = gidx == 0 || gidx == n - 1 || n < 3;
+        return v && (e || (p >= 2 && p <= T - 3));
+    };
+    const bool needC = needC_at(pos, gi);
+    State<NM, D> LS, RS;
+    Prim<NM, D> PLS, PRS;
+    if (needC) {
+        Prim<NM, D> lo, hi;
+        if (!end) {
+            sm_get<NM, D>(sm, NT, t - s, 0, lo);
+            sm_get<NM, D>(sm, NT, t + s, 0, hi);
+        }
+        stage_c<NM, D>(M, U, A, Ph, lo, hi, end, LS, RS, PLS, PRS);
+    }
+    __syncthreads();
+    if (needC) {
+        sm_put<NM, D>(sm, NT, t, 0, LS);
+        sm_put<NM, D>(sm, NT, t, kStateVars(NM, D), PLS);
+    }
+    __syncthreads();
+
+    // ---- stage D: face between this cell and the next one
+    const bool needD = needC && pos + 1 <= T - 1 && gi + 1 < n && needC_at(pos + 1, gi + 1);
+    FaceD<NM, D> fd;
+    if (needD) {
+        State<NM, D> UR;
+        Prim<NM, D> PR;
+        sm_get<NM, D>(sm, NT, t + s, 0, UR);
+        sm_get<NM, D>(sm, NT, t + s, kStateVars(NM, D), PR);
+        if (!stage_d<NM, D>(M, RS, PRS, UR, PR, DIR, fd)) atomicOr(err, kErrNonFinite);
+    }
+    __syncthreads();
+    if (needD) sm_put<NM, D>(sm, NT, t, fd);
+    __syncthreads();
+
+    // ---- stage E: the outputs
+    if (valid && pos >= 3 && pos <= T - 4) {
+        FaceD<NM, D> lo;
+        if (!first) sm_get<NM, D>(sm, NT, t - s, lo);
+        State<NM, D> Un;
+        stage_e<NM, D>(M, U, A, first ? nullptr : &lo, last ? nullptr : &fd, first, last, dt, dx, Un);
+        store_cell<NM, D>(out, g.ncell, cell, Un);
+    }
+}
+
+// ---- CFL ------------------------------------------------------------------------
+__device__ __forceinline__ double warp_min(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+template<int NM, int D>
+__global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st, Grid g, Mats M, double cfl,
+                                                  int unsplit, double* __restrict__ blockmin)
+{
+    __shared__ double red[32];
+    double best = HUGE_VAL;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell; i += stride) {
+        State<NM, D> U;
+        Prim<NM, D> P;
+        load_cell<NM, D>(st, g.ncell, i, U);
+        cons_to_prim<NM, D>(M, U, P);
+        best = dmin(best, cfl_candidate<NM, D>(M, U, P, g.dx, cfl, unsplit != 0));
+    }
+    best = warp_min(best);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        const int nw = blockDim.x >> 5;
+        double v = threadIdx.x < nw ? red[threadIdx.x] : HUGE_VAL;
+        v = warp_min(v);
+        if (threadIdx.x == 0) blockmin[blockIdx.x] = v;
+    }
+}
+
+// ---- boundary fill (dim::apply_boundary_conditions, src/dim/solver/advance/
+// boundary.hpp:165-226) ----------------------------------------------------------
+//
+// Every boundary cell copies its source cell (each boundary axis shifted one
+// cell inward), flipping the normal momentum on reflective sides; cells named
+// nonreflective by boundary_name_for_cell (:23-41) take
+// local_nonreflective_state (:113-163).  For axes with N >= 4 (N >= 3 without
+// nonreflective sides) every cell read is an interior cell, so the
+// reference's serial in-place loop is order-independent and one thread per
+// boundary cell reproduces it; otherwise the host runs the serial variant.
+template<int NM, int D>
+__device__ void bc_cell(const Grid& g, const Mats& M, double* st, const int* idx, long long linear)
+{
+    int src[3] = {0, 0, 0};
+    bool is_boundary = false;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        src[a] = idx[a];
+        if (g.N[a] <= 1) continue;
+        if (idx[a] == 0) { src[a] = 1; is_boundary = true; }
+        else if (idx[a] == g.N[a] - 1) { src[a] = g.N[a] - 2; is_boundary = true; }
+    }
+    if (!is_boundary) return;
+    int bc = DIMGPU_BC_TRANSMISSIVE;
+#pragma unroll
+    for (int a = 0; a < D; ++a) {
+        if (idx[a] == 0) { bc = g.bc_lo[a]; break; }
+        if (idx[a] == g.N[a] - 1) { bc = g.bc_hi[a]; break; }
+    }
+    long long src_lin = 0;
+#pragma unroll
+    for (int a = 0; a < D; ++a) src_lin += (long long)src[a] * g.stride[a];
+    State<NM, D> U;
+    int q;
+    if (bc == DIMGPU_BC_NONREFLECTIVE) {
+        int second[3] = {src[0], src[1], src[2]};
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            if (idx[a] == 0 && g.N[a] > 2) second[a] = 2;
+            else if (idx[a] == g.N[a] - 1 && g.N[a] > 2) second[a] = g.N[a] - 3;
+        }
+        long long sec_lin = 0;
+#pragma unroll
+        for (int a = 0; a < D; ++a) sec_lin += (long long)second[a] * g.stride[a];
+        State<NM, D> first, sec, ex;
+        // plain loads: the serial variant reads cells this launch rewrites
+        q = 0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) { first.m[k] = st[q * g.ncell + src_lin]; sec.m[k] = st[q * g.ncell + sec_lin]; ++q; }
+#pragma unroll
+        for (int d = 0; d < D; ++d) { first.mom[d] = st[q * g.ncell + src_lin]; sec.mom[d] = st[q * g.ncell + sec_lin]; ++q; }
+        first.E = st[q * g.ncell + src_lin]; sec.E = st[q * g.ncell + sec_lin]; ++q;
+#pragma unroll
+        for (int k = 0; k < NM - 1; ++k) { first.a[k] = st[q * g.ncell + src_lin]; sec.a[k] = st[q * g.ncell + sec_lin]; ++q; }
+        U = first;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) ex.m[k] = first.m[k] + (first.m[k] - sec.m[k]);
+#pragma unroll
+        for (int d = 0; d < D; ++d) ex.mom[d] = first.mom[d] + (first.mom[d] - sec.mom[d]);
+        ex.E = first.E + (first.E - sec.E);
+        int axis = 0;
+#pragma unroll
+        for (int a = D - 1; a >= 0; --a)
+            if (idx[a] == 0 || idx[a] == g.N[a] - 1) axis = a;
+        const int outward = (idx[axis] == 0) ? -1 : 1;
+        const double ex_rho = dmax(total_density<NM, D>(ex), 1e-12);
+        double ex_mom_axis = 0.0;
+#pragma unroll
+        for (int d = 0; d < D; ++d)
+            if (d == axis) ex_mom_axis = ex.mom[d];
+        const double ex_un = outward * safe_div(ex_mom_axis, ex_rho);
+        if (ex_un > 0.0) {
+            const double rho = dmax(total_density<NM, D>(U), 1e-12);
+            double b = 0.0, af = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) b += U.mom[d] * U.mom[d];
+#pragma unroll
+            for (int d = 0; d < D; ++d)
+                if (d == axis) U.mom[d] = ex.mom[d];
+#pragma unroll
+            for (int d = 0; d < D; ++d) af += U.mom[d] * U.mom[d];
+            U.E += 0.5 * (af - b) / rho;
+        }
+        repair_state<NM, D>(M, U);
+    }
+    else {
+        q = 0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) U.m[k] = st[(q++) * g.ncell + src_lin];
+#pragma unroll
+        for (int d = 0; d < D; ++d) U.mom[d] = st[(q++) * g.ncell + src_lin];
+        U.E = st[(q++) * g.ncell + src_lin];
+#pragma unroll
+        for (int k = 0; k < NM - 1; ++k) U.a[k] = st[(q++) * g.ncell + src_lin];
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            if ((idx[a] == 0 && g.bc_lo[a] == DIMGPU_BC_REFLECTIVE) ||
+                (idx[a] == g.N[a] - 1 && g.bc_hi[a] == DIMGPU_BC_REFLECTIVE))
+                U.mom[a] *= -1.0;
+        }
+    }
+    q = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) st[(q++) * g.ncell + linear] = U.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) st[(q++) * g.ncell + linear] = U.mom[d];
+    st[(q++) * g.ncell + linear] = U.E;
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) st[(q++) * g.ncell + linear] = U.a[k];
+}
+
+// The boundary shell as planes: plane 2a+side holds the cells with
+// idx[a] == (side ? N[a]-1 : 0) whose lower axes b < a are interior, so
+// every boundary cell is visited exactly once.
+template<int NM, int D>
+__global__ void __launch_bounds__(256) bc_kernel(double* st, Grid g, Mats M, long long plane0, long long plane1,
+                                                 long long plane2)
+{
+    const long long count[3] = {plane0, plane1, plane2};
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int a = 0;
+    while (a < D && i >= 2 * count[a]) { i -= 2 * count[a]; ++a; }
+    if (a >= D) return;
+    const int side = (int)(i / count[a]);
+    long long r = i % count[a];
+    int idx[3] = {0, 0, 0};
+#pragma unroll
+    for (int b = 0; b < D; ++b) {
+        if (b == a) continue;
+        // lower axes: interior cells only (an axis with N == 1 has no boundary)
+        const bool inner = b < a && g.N[b] != 1;
+        const int ext = inner ? (g.N[b] - 2) : g.N[b];
+        idx[b] = (int)(r % ext) + (inner ? 1 : 0);
+        r /= ext;
+    }
+    idx[a] = side ? g.N[a] - 1 : 0;
+    long long linear = 0;
+#pragma unroll
+    for (int b = 0; b < D; ++b) linear += (long long)idx[b] * g.stride[b];
+    bc_cell<NM, D>(g, M, st, idx, linear);
+}
+
+// The reference's literal serial order, for grids where it matters.
+template<int NM, int D>
+__global__ void bc_serial_kernel(double* st, Grid g, Mats M)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    for (long long linear = 0; linear < g.ncell; ++linear) {
+        int idx[3] = {0, 0, 0};
+        long long s = 1;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            idx[a] = (int)((linear / s) % g.N[a]);
+            s *= g.N[a];
+        }
+        bc_cell<NM, D>(g, M, st, idx, linear);
+    }
+}
+
+// ---- unsplit accumulation (src/dim/solver/advance_step.hpp:198-222) -------------
+template<int NM, int D>
+__global__ void __launch_bounds__(256) accumulate_kernel(double* __restrict__ acc, const double* __restrict__ dir_state,
+                                                         const double* __restrict__ base, Grid g, Mats M)
+{
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= g.ncell) return;
+    State<NM, D> a, d, b;
+    load_cell<NM, D>(acc, g.ncell, i, a);
+    load_cell<NM, D>(dir_state, g.ncell, i, d);
+    load_cell<NM, D>(base, g.ncell, i, b);
+#pragma unroll
+    for (int k = 0; k < NM; ++k) a.m[k] += d.m[k] - b.m[k];
+#pragma unroll
+    for (int q = 0; q < D; ++q) a.mom[q] += d.mom[q] - b.mom[q];
+    a.E += d.E - b.E;
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) a.a[k] += d.a[k] - b.a[k];
+    repair_state<NM, D>(M, a);
+    store_cell<NM, D>(acc, g.ncell, i, a);
+}
+
+// ---- conservation totals (compute_dim_conservation_totals,
+// src/app/io/conservation_report.hpp:188-218): per-block partial sums ------------
+template<int NM, int D>
+__global__ void __launch_bounds__(256) totals_kernel(const double* __restrict__ st, Grid g, double volume,
+                                                     double* __restrict__ partial)
+{
+    constexpr int NV = NM + 1 + D + 1;
+    __shared__ double red[NV][256];
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell; i += stride) {
+        double cell_mass = 0.0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) {
+            const double part = st[k * g.ncell + i] * volume;
+            acc[k] += part;
+            cell_mass += part;
+        }
+        acc[NM] += cell_mass;
+#pragma unroll
+        for (int d = 0; d < D; ++d) acc[NM + 1 + d] += st[(NM + d) * g.ncell + i] * volume;
+        acc[NM + 1 + D] += st[(NM + D) * g.ncell + i] * volume;
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) red[v][threadIdx.x] = acc[v];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) partial[(long long)blockIdx.x * NV + v] = red[v][0];
+    }
+}
+
+// ---- launchers ---------------------------------------------------------------------
+template<int NM, int D, int DIR>
+cudaError_t launch_sweep_dir(const Grid& g, const Mats& M, Tile tile, const double* in, double* out,
+                             const double* dt, int* err, cudaStream_t s)
+{
+    const int n = g.N[DIR];
+    const int T = tile.T, W = tile.W;
+    const int ntile = (n + (T - 6) - 1) / (T - 6);
+    long long nblocks;
+    int ngx = 1;
+    if (DIR == 0) {
+        const long long nlines = g.ncell / g.N[0];
+        nblocks = (long long)ntile * ((nlines + W - 1) / W);
+    }
+    else {
+        ngx = (g.N[0] + W - 1) / W;
+        const long long other = g.ncell / ((long long)g.N[0] * g.N[DIR]);
+        nblocks = (long long)ngx * ntile * other;
+    }
+    const size_t smem = sizeof(double) * (size_t)kSweepSmemVars(NM, D) * (size_t)(T * W);
+    auto kern = sweep_kernel<NM, D, DIR>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err);
+    return cudaGetLastError();
+}
+
+template<int NM, int D>
+cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const double* in, double* out,
+                         const double* dt, int* err, cudaStream_t s)
+{
+    if (tile.T < 8 || tile.W < 1 || tile.T * tile.W > 256) return cudaErrorInvalidValue;
+    if (dir == 0) return launch_sweep_dir<NM, D, 0>(g, M, tile, in, out, dt, err, s);
+    if constexpr (D >= 2) {
+        if (dir == 1) return launch_sweep_dir<NM, D, 1>(g, M, tile, in, out, dt, err, s);
+    }
+    if constexpr (D >= 3) {
+        if (dir == 2) return launch_sweep_dir<NM, D, 2>(g, M, tile, in, out, dt, err, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template<int NM, int D>
+cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s)
+{
+    long long nb = (g.ncell + 255) / 256;
+    if (nb > max_blocks) nb = max_blocks;
+    if (nb < 1) nb = 1;
+    *nblocks = (int)nb;
+    cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, blockmin);
+    return cudaGetLastError();
+}
+
+template<int NM, int D>
+cudaError_t launch_bc(const Grid& g, const Mats& M, double* state, cudaStream_t s)
+{
+    // N == 2 makes a source cell a boundary cell; with a nonreflective side,
+    // N == 3 on any axis makes the extrapolation's second cell one.
+    bool serial = false, nonreflective = false, three = false;
+    for (int a = 0; a < D; ++a) {
+        if (g.N[a] == 2) serial = true;
+        if (g.N[a] == 3) three = true;
+        if (g.bc_lo[a] == DIMGPU_BC_NONREFLECTIVE || g.bc_hi[a] == DIMGPU_BC_NONREFLECTIVE) nonreflective = true;
+    }
+    if (nonreflective && three) serial = true;
+    if (serial) {
+        bc_serial_kernel<NM, D><<<1, 1, 0, s>>>(state, g, M);
+        return cudaGetLastError();
+    }
+    long long plane[3] = {0, 0, 0};
+    long long total = 0;
+    for (int a = 0; a < D; ++a) {
+        if (g.N[a] <= 1) continue;
+        long long c = 1;
+        for (int b = 0; b < D; ++b) {
+            if (b == a) continue;
+            c *= (b < a && g.N[b] != 1) ? (long long)(g.N[b] - 2) : (long long)g.N[b];
+        }
+        plane[a] = c;
+        total += 2 * c;
+    }
+    if (total == 0) return cudaSuccess;
+    bc_kernel<NM, D><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(state, g, M, plane[0], plane[1], plane[2]);
+    return cudaGetLastError();
+}
+
+template<int NM, int D>
+cudaError_t launch_accumulate(const Grid& g, const Mats& M, double* accum, const double* dir_state,
+                              const double* base, cudaStream_t s)
+{
+    accumulate_kernel<NM, D><<<(unsigned)((g.ncell + 255) / 256), 256, 0, s>>>(accum, dir_state, base, g, M);
+    return cudaGetLastError();
+}
+
+template<int NM, int D>
+cudaError_t launch_totals(const Grid& g, const double* state, double volume, double* partial, int max_blocks,
+                          int* nblocks, cudaStream_t s)
+{
+    long long nb = (g.ncell + 255) / 256;
+    if (nb > max_blocks) nb = max_blocks;
+    if (nb < 1) nb = 1;
+    *nblocks = (int)nb;
+    totals_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, volume, partial);
+    return cudaGetLastError();
+}
+
+#define DIMGPU_INSTANTIATE_D(NM, D)                                                                          \
+    template cudaError_t launch_sweep<NM, D>(const Grid&, const Mats&, int, Tile, const double*, double*,    \
+                                             const double*, int*, cudaStream_t);                             \
+    template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
+                                           int, int*, cudaStream_t);                                         \
+    template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \
+    template cudaError_t launch_accumulate<NM, D>(const Grid&, const Mats&, double*, const double*,          \
+                                                  const double*, cudaStream_t);                              \
+    template cudaError_t launch_totals<NM, D>(const Grid&, const double*, double, double*, int, int*,        \
+                                              cudaStream_t);
+
+#define DIMGPU_INSTANTIATE(NM)   \
+    DIMGPU_INSTANTIATE_D(NM, 1)  \
+    DIMGPU_INSTANTIATE_D(NM, 2)  \
+    DIMGPU_INSTANTIATE_D(NM, 3)
+
+}  // namespace dimgpu

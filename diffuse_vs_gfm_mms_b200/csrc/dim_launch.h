@@ -1,0 +1,61 @@
+// dim_launch.h — host-side declarations of the kernel launchers.  The
+// launchers are templates over the material count NM and the dimension D,
+// defined in dim_kernels.cuh and instantiated per NM in inst_nm*.cu.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "dim_physics.h"
+
+namespace dimgpu {
+
+// Error bits written by the kernels into the session's flag word.
+enum : int {
+    kErrNonFinite = 1,  // hllc_flux_normal's require_positive would throw
+    kErrDt = 2,         // CFL step is not positive and finite
+};
+
+struct Grid {
+    int N[3];
+    long long ncell;
+    long long stride[3];  // 1, Nx, Nx*Ny
+    double dx[3];
+    int bc_lo[3], bc_hi[3];
+};
+
+// Tile shape of the sweep kernel: T cells along the line (T - 6 of them are
+// outputs, the other 6 the stencil halo), W lines per CTA.
+struct Tile {
+    int T;
+    int W;
+};
+
+template<int NM, int D>
+cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const double* in, double* out,
+                         const double* dt, int* err, cudaStream_t s);
+
+// Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
+template<int NM, int D>
+cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s);
+
+// dt = min(dt_max, min(blockmin)), written to dt[0] and hist[0] (hist may be null).
+cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_max, double* dt,
+                                double* hist, int* err, cudaStream_t s);
+
+template<int NM, int D>
+cudaError_t launch_bc(const Grid& g, const Mats& M, double* state, cudaStream_t s);
+
+// accum += dir - base, then repair_state, for the unsplit update.
+template<int NM, int D>
+cudaError_t launch_accumulate(const Grid& g, const Mats& M, double* accum, const double* dir_state,
+                              const double* base, cudaStream_t s);
+
+// Per-block partial conservation sums: nmat + 1 + D + 1 values per block.
+template<int NM, int D>
+cudaError_t launch_totals(const Grid& g, const double* state, double volume, double* partial,
+                          int max_blocks, int* nblocks, cudaStream_t s);
+
+int sweep_smem_doubles(int nmat, int dim);
+
+}  // namespace dimgpu

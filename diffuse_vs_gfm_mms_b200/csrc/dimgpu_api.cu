@@ -1,0 +1,596 @@
+// dimgpu_api.cu — the C-ABI (include/dimgpu.h): sessions owning the
+// device-resident SoA state, the step orchestration of dim::advance_one_step
+// (src/dim/solver/advance_step.hpp:150-270) and the stateless drop-in call.
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "dim_launch.h"
+#include "dimgpu.h"
+
+using namespace dimgpu;
+
+namespace {
+
+constexpr int kMaxCflBlocks = 148 * 8;
+constexpr int kHistCap = 4096;
+constexpr int kTotalsBlocks = 1024;
+
+enum Kind { kSweep = 0, kCfl = 1, kBoundary = 2, kOther = 3 };
+
+thread_local std::string g_err = "";
+
+int fail(std::string* where, int code, const std::string& msg)
+{
+    if (where) *where = msg;
+    g_err = msg;
+    return code;
+}
+
+#define DISPATCH_ND(nm, dim, ...)                                                   \
+    switch ((nm) * 10 + (dim)) {                                                    \
+        case 11: { constexpr int NM = 1, D = 1; __VA_ARGS__; } break;               \
+        case 12: { constexpr int NM = 1, D = 2; __VA_ARGS__; } break;               \
+        case 13: { constexpr int NM = 1, D = 3; __VA_ARGS__; } break;               \
+        case 21: { constexpr int NM = 2, D = 1; __VA_ARGS__; } break;               \
+        case 22: { constexpr int NM = 2, D = 2; __VA_ARGS__; } break;               \
+        case 23: { constexpr int NM = 2, D = 3; __VA_ARGS__; } break;               \
+        case 31: { constexpr int NM = 3, D = 1; __VA_ARGS__; } break;               \
+        case 32: { constexpr int NM = 3, D = 2; __VA_ARGS__; } break;               \
+        case 33: { constexpr int NM = 3, D = 3; __VA_ARGS__; } break;               \
+        case 41: { constexpr int NM = 4, D = 1; __VA_ARGS__; } break;               \
+        case 42: { constexpr int NM = 4, D = 2; __VA_ARGS__; } break;               \
+        case 43: { constexpr int NM = 4, D = 3; __VA_ARGS__; } break;               \
+        default: e = cudaErrorInvalidValue; break;                                  \
+    }
+
+__device__ __forceinline__ double warp_min_f(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = dmin(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// dt = std::min(dt_max, every candidate) (src/dim/solver/cfl.hpp:43-63): the
+// min of non-NaN values is independent of the order.
+__global__ void cfl_finalize_kernel(const double* __restrict__ blockmin, int nb, double dt_max,
+                                    double* __restrict__ dt, double* __restrict__ hist, int* __restrict__ err)
+{
+    __shared__ double red[32];
+    double v = HUGE_VAL;
+    for (int i = threadIdx.x; i < nb; i += blockDim.x) v = dmin(v, blockmin[i]);
+    v = warp_min_f(v);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = dmin(m, red[w]);
+        const double d = dmin(dt_max, m);
+        dt[0] = d;
+        if (hist) hist[0] = d;
+        if (!(d > 0.0) || !fin(d)) atomicOr(err, kErrDt);
+    }
+}
+
+}  // namespace
+
+namespace dimgpu {
+
+cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_max, double* dt, double* hist,
+                                int* err, cudaStream_t s)
+{
+    cfl_finalize_kernel<<<1, 256, 0, s>>>(blockmin, nblocks, dt_max, dt, hist, err);
+    return cudaGetLastError();
+}
+
+int sweep_smem_doubles(int nmat, int dim) { return (2 * nmat + dim) + (2 * nmat + dim + 1); }
+
+}  // namespace dimgpu
+
+struct dimgpu_session {
+    dimgpu_desc desc{};
+    Mats M{};
+    Grid g{};
+    int V = 0;
+    long long ncell = 0;
+    double* buf[3] = {nullptr, nullptr, nullptr};
+    int cur = 0;
+    double* blockmin = nullptr;
+    double* dt = nullptr;
+    double* hist = nullptr;
+    double* partial = nullptr;
+    int* err = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    Tile tile[3] = {{128, 1}, {64, 4}, {64, 4}};
+    std::string msg;
+    // profiling
+    bool profiling = false;
+    struct Rec { int kind; cudaEvent_t a, b; };
+    std::vector<Rec> recs;
+    std::vector<cudaEvent_t> pool;
+    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int pending = 0;  // steps enqueued since the last collection
+};
+
+namespace {
+
+cudaEvent_t pool_get(dimgpu_session* s)
+{
+    if (!s->pool.empty()) {
+        cudaEvent_t e = s->pool.back();
+        s->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+struct ProfScope {
+    dimgpu_session* s;
+    int kind;
+    cudaEvent_t a = nullptr;
+    ProfScope(dimgpu_session* s_, int k) : s(s_), kind(k)
+    {
+        if (s->profiling) {
+            a = pool_get(s);
+            cudaEventRecord(a, s->stream);
+        }
+    }
+    ~ProfScope()
+    {
+        if (s->profiling) {
+            cudaEvent_t b = pool_get(s);
+            cudaEventRecord(b, s->stream);
+            s->recs.push_back({kind, a, b});
+        }
+    }
+};
+
+void prof_drain(dimgpu_session* s)
+{
+    if (s->recs.empty()) return;
+    cudaStreamSynchronize(s->stream);
+    for (auto& r : s->recs) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        s->prof[2 * r.kind] += ms;
+        s->prof[2 * r.kind + 1] += 1.0;
+        s->pool.push_back(r.a);
+        s->pool.push_back(r.b);
+    }
+    s->recs.clear();
+}
+
+int cuda_fail(dimgpu_session* s, cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation)
+        return fail(s ? &s->msg : nullptr, DIMGPU_E_OOM, std::string(what) + ": out of device memory");
+    return fail(s ? &s->msg : nullptr, DIMGPU_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+int validate_desc(const dimgpu_desc* d, std::string* where)
+{
+    if (!d) return fail(where, DIMGPU_E_INVALID_ARG, "null descriptor");
+    if (d->dim < 1 || d->dim > 3) return fail(where, DIMGPU_E_INVALID_ARG, "dim must be 1, 2 or 3");
+    if (d->nmat < 1 || d->nmat > DIMGPU_MAX_MATERIALS)
+        return fail(where, DIMGPU_E_INVALID_ARG, "dim::EOSParams: nmat must be 1..4");
+    for (int a = 0; a < 3; ++a) {
+        const int n = d->N[a];
+        if (a < d->dim && n < 1) return fail(where, DIMGPU_E_INVALID_ARG, "dim::total_cells: grid size must be positive");
+        if (a >= d->dim && n != 1) return fail(where, DIMGPU_E_INVALID_ARG, "unused axes must have N = 1");
+        if (a < d->dim && !(d->dx[a] > 0.0))
+            return fail(where, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: grid spacing must be positive");
+    }
+    for (int k = 0; k < d->nmat; ++k) {
+        const int kind = d->mat[k].kind;
+        if (kind != DIMGPU_EOS_IDEAL_GAS && kind != DIMGPU_EOS_STIFFENED_GAS)
+            return fail(where, DIMGPU_E_UNSUPPORTED_EOS,
+                        "material " + std::to_string(k) + ": only ideal_gas and stiffened_gas run on the GPU");
+        if (!(d->mat[k].gamma > 1.0)) return fail(where, DIMGPU_E_INVALID_ARG, "dim::EOSParams: gamma must be > 1");
+    }
+    if (d->lambda_model < 0 || d->lambda_model > 2)
+        return fail(where, DIMGPU_E_INVALID_ARG, "dim::alpha_rhs_coefficients: unknown lambda model");
+    if (d->precision != DIMGPU_PRECISION_FP64)
+        return fail(where, DIMGPU_E_UNSUPPORTED, "this build runs precision FP64 only");
+    if (d->time_update != DIMGPU_TIME_SPLIT && d->time_update != DIMGPU_TIME_UNSPLIT)
+        return fail(where, DIMGPU_E_INVALID_ARG, "time_update must be split or unsplit");
+    return DIMGPU_OK;
+}
+
+int check_err(dimgpu_session* s)
+{
+    int h = 0;
+    cudaError_t e = cudaMemcpyAsync(&h, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "step");
+    if (h) {
+        cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+        if (h & kErrNonFinite)
+            return fail(&s->msg, DIMGPU_E_NONFINITE, "dim::hllc_flux_normal: invalid density or pressure (non-finite)");
+        if (h & kErrDt) return fail(&s->msg, DIMGPU_E_NONFINITE, "run_dim_case: non-positive timestep");
+    }
+    return DIMGPU_OK;
+}
+
+// CFL dt of buf[cur] into s->dt (and hist slot).
+cudaError_t run_cfl(dimgpu_session* s, double cfl, double dt_max, double* hist)
+{
+    cudaError_t e = cudaSuccess;
+    int nb = 1;
+    {
+        ProfScope p(s, kCfl);
+        const bool unsplit = s->desc.time_update == DIMGPU_TIME_UNSPLIT;
+        DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                    e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks,
+                                          &nb, s->stream));
+    }
+    if (e != cudaSuccess) return e;
+    ProfScope p(s, kOther);
+    return launch_cfl_finalize(s->blockmin, nb, dt_max, s->dt, hist, s->err, s->stream);
+}
+
+cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out)
+{
+    cudaError_t e = cudaSuccess;
+    ProfScope p(s, kSweep);
+    DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                e = launch_sweep<NM, D>(s->g, s->M, dir, s->tile[dir], in, out, s->dt, s->err, s->stream));
+    return e;
+}
+
+cudaError_t run_bc(dimgpu_session* s, double* st)
+{
+    cudaError_t e = cudaSuccess;
+    ProfScope p(s, kBoundary);
+    DISPATCH_ND(s->desc.nmat, s->desc.dim, e = launch_bc<NM, D>(s->g, s->M, st, s->stream));
+    return e;
+}
+
+// The sweeps and boundary fills of one step, dt already in s->dt
+// (advance_split_directions / advance_unsplit_directions,
+// src/core/fv/directional_update.hpp:8-44).
+cudaError_t run_directions(dimgpu_session* s)
+{
+    cudaError_t e = cudaSuccess;
+    const int D = s->desc.dim;
+    if (s->desc.time_update == DIMGPU_TIME_SPLIT) {
+        for (int dir = 0; dir < D && e == cudaSuccess; ++dir) {
+            if (s->g.N[dir] > 1) {  // a line of one cell is copied unchanged (sweep_core.hpp:35-38)
+                e = run_sweep(s, dir, s->buf[s->cur], s->buf[1 - s->cur]);
+                s->cur = 1 - s->cur;
+            }
+            if (e == cudaSuccess) e = run_bc(s, s->buf[s->cur]);
+        }
+        return e;
+    }
+    // unsplit: acc = base; per axis acc += sweep(base) - base, repair; one fill
+    const int base = s->cur, acc = 1 - s->cur;
+    const size_t bytes = sizeof(double) * (size_t)s->V * (size_t)s->ncell;
+    e = cudaMemcpyAsync(s->buf[acc], s->buf[base], bytes, cudaMemcpyDeviceToDevice, s->stream);
+    for (int dir = 0; dir < D && e == cudaSuccess; ++dir) {
+        const double* dstate = s->buf[base];
+        if (s->g.N[dir] > 1) {
+            e = run_sweep(s, dir, s->buf[base], s->buf[2]);
+            dstate = s->buf[2];
+        }
+        if (e != cudaSuccess) break;
+        ProfScope p(s, kOther);
+        DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                    e = launch_accumulate<NM, D>(s->g, s->M, s->buf[acc], dstate, s->buf[base], s->stream));
+    }
+    if (e == cudaSuccess) e = run_bc(s, s->buf[acc]);
+    s->cur = acc;
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dimgpu_components(const dimgpu_desc* desc) { return desc ? 2 * desc->nmat + desc->dim : 0; }
+
+const char* dimgpu_last_error(const dimgpu_session* s)
+{
+    if (s) return s->msg.c_str();
+    return g_err.c_str();
+}
+
+int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
+{
+    if (!out) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    int rc = validate_desc(desc, nullptr);
+    if (rc) return rc;
+    auto* s = new dimgpu_session();
+    s->desc = *desc;
+    int kind[kMaxMat];
+    double gam[kMaxMat], pinf[kMaxMat];
+    for (int k = 0; k < desc->nmat; ++k) {
+        kind[k] = desc->mat[k].kind;
+        gam[k] = desc->mat[k].gamma;
+        pinf[k] = desc->mat[k].p_inf;
+    }
+    fill_mats(s->M, desc->nmat, kind, gam, pinf, desc->lambda_model, desc->alpha_source_floor);
+    s->V = 2 * desc->nmat + desc->dim;
+    s->ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        s->g.N[a] = desc->N[a];
+        s->g.dx[a] = desc->dx[a];
+        s->g.bc_lo[a] = desc->bc_lo[a];
+        s->g.bc_hi[a] = desc->bc_hi[a];
+        s->ncell *= desc->N[a];
+    }
+    s->g.ncell = s->ncell;
+    s->g.stride[0] = 1;
+    s->g.stride[1] = desc->N[0];
+    s->g.stride[2] = (long long)desc->N[0] * desc->N[1];
+    // y / z sweeps of narrow grids: fewer lines per CTA, longer segments
+    for (int dir = 1; dir < 3; ++dir)
+        if (desc->N[0] < 4) s->tile[dir] = {128, 1};
+
+    const size_t bytes = sizeof(double) * (size_t)s->V * (size_t)s->ncell;
+    cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
+    s->stream = s->own_stream;
+    const int nbuf = desc->time_update == DIMGPU_TIME_UNSPLIT ? 3 : 2;
+    for (int b = 0; b < nbuf && e == cudaSuccess; ++b) e = cudaMalloc(&s->buf[b], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&s->blockmin, sizeof(double) * kMaxCflBlocks);
+    if (e == cudaSuccess) e = cudaMalloc(&s->dt, sizeof(double) * 2);
+    if (e == cudaSuccess) e = cudaMalloc(&s->hist, sizeof(double) * kHistCap);
+    if (e == cudaSuccess) e = cudaMalloc(&s->partial, sizeof(double) * kTotalsBlocks * (DIMGPU_MAX_MATERIALS + 5));
+    if (e == cudaSuccess) e = cudaMalloc(&s->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+        rc = cuda_fail(nullptr, e, "dimgpu_create");
+        dimgpu_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return DIMGPU_OK;
+}
+
+int dimgpu_destroy(dimgpu_session* s)
+{
+    if (!s) return DIMGPU_OK;
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (auto& r : s->recs) {
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    for (auto ev : s->pool) cudaEventDestroy(ev);
+    for (int b = 0; b < 3; ++b) cudaFree(s->buf[b]);
+    cudaFree(s->blockmin);
+    cudaFree(s->dt);
+    cudaFree(s->hist);
+    cudaFree(s->partial);
+    cudaFree(s->err);
+    if (s->own_stream) cudaStreamDestroy(s->own_stream);
+    delete s;
+    return DIMGPU_OK;
+}
+
+int dimgpu_upload(dimgpu_session* s, const double* soa, size_t count)
+{
+    if (!s || !soa) return fail(s ? &s->msg : nullptr, DIMGPU_E_INVALID_ARG, "null argument");
+    if (count != (size_t)s->V * (size_t)s->ncell)
+        return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::advance_one_step: grid size mismatch");
+    cudaError_t e = cudaMemcpyAsync(s->buf[s->cur], soa, sizeof(double) * count, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? DIMGPU_OK : cuda_fail(s, e, "dimgpu_upload");
+}
+
+int dimgpu_download(dimgpu_session* s, double* soa, size_t count)
+{
+    if (!s || !soa) return fail(s ? &s->msg : nullptr, DIMGPU_E_INVALID_ARG, "null argument");
+    if (count != (size_t)s->V * (size_t)s->ncell)
+        return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dimgpu_download: buffer size mismatch");
+    cudaError_t e = cudaMemcpyAsync(soa, s->buf[s->cur], sizeof(double) * count, cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? DIMGPU_OK : cuda_fail(s, e, "dimgpu_download");
+}
+
+int dimgpu_compute_dt_cfl(dimgpu_session* s, double cfl, double dt_max, double* dt_out)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (!(cfl > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: cfl must be positive");
+    if (!(dt_max > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: dt_max must be positive");
+    cudaError_t e = run_cfl(s, cfl, dt_max, nullptr);
+    double h = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, s->dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_compute_dt_cfl");
+    cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);  // dt <= 0 is the caller's decision here
+    if (dt_out) *dt_out = h;
+    return DIMGPU_OK;
+}
+
+int dimgpu_sweep_direction(dimgpu_session* s, int dir, double dt)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (dir < 0 || dir >= s->desc.dim) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "sweep direction out of range");
+    cudaError_t e = cudaMemcpyAsync(s->dt, &dt, sizeof(double), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess && s->g.N[dir] > 1) {
+        e = run_sweep(s, dir, s->buf[s->cur], s->buf[1 - s->cur]);
+        s->cur = 1 - s->cur;
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_sweep_direction");
+    return check_err(s);
+}
+
+int dimgpu_apply_boundary_conditions(dimgpu_session* s)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    cudaError_t e = run_bc(s, s->buf[s->cur]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    return e == cudaSuccess ? DIMGPU_OK : cuda_fail(s, e, "dimgpu_apply_boundary_conditions");
+}
+
+int dimgpu_step(dimgpu_session* s, double cfl, double dt_max, double* dt_out, dimgpu_phase_times* times)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (!(cfl > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: cfl must be positive");
+    if (!(dt_max > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: dt_max must be positive");
+    const bool was = s->profiling;
+    double before[8];
+    if (times) {
+        prof_drain(s);
+        std::memcpy(before, s->prof, sizeof before);
+        s->profiling = true;
+    }
+    cudaError_t e = run_cfl(s, cfl, dt_max, nullptr);
+    if (e == cudaSuccess) e = run_directions(s);
+    double h = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, s->dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (times) {
+        prof_drain(s);
+        s->profiling = was;
+        times->cfl_ms = s->prof[2 * kCfl] - before[2 * kCfl] + s->prof[2 * kOther] - before[2 * kOther];
+        times->sweep_ms = s->prof[2 * kSweep] - before[2 * kSweep];
+        times->boundary_ms = s->prof[2 * kBoundary] - before[2 * kBoundary];
+        if (!was) std::memset(s->prof, 0, sizeof s->prof);
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_step");
+    if (dt_out) *dt_out = h;
+    int hflag = 0;
+    e = cudaMemcpyAsync(&hflag, s->err, sizeof(int), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_step");
+    if (hflag & kErrNonFinite) return check_err(s);
+    if (hflag) cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);  // dt <= 0: returned to the caller
+    return DIMGPU_OK;
+}
+
+int dimgpu_enqueue_steps(dimgpu_session* s, int n, double cfl, double dt_max)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (n < 0) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "negative step count");
+    if (!(cfl > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: cfl must be positive");
+    if (!(dt_max > 0.0)) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: dt_max must be positive");
+    if (s->pending + n > kHistCap)
+        return fail(&s->msg, DIMGPU_E_INVALID_ARG, "more than 4096 steps enqueued: call dimgpu_collect first");
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < n && e == cudaSuccess; ++k) {
+        e = run_cfl(s, cfl, dt_max, s->hist + s->pending);
+        if (e == cudaSuccess) e = run_directions(s);
+        if (e == cudaSuccess) ++s->pending;
+    }
+    return e == cudaSuccess ? DIMGPU_OK : cuda_fail(s, e, "dimgpu_enqueue_steps");
+}
+
+int dimgpu_collect(dimgpu_session* s, double* dt_out, int capacity, int* count)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    const int n = s->pending;
+    s->pending = 0;
+    if (count) *count = n;
+    cudaError_t e = cudaSuccess;
+    if (dt_out && n > 0) {
+        if (capacity < n) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "dimgpu_collect: dt_out too small");
+        e = cudaMemcpyAsync(dt_out, s->hist, sizeof(double) * n, cudaMemcpyDeviceToHost, s->stream);
+    }
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_collect");
+    return check_err(s);
+}
+
+int dimgpu_steps(dimgpu_session* s, int n, double cfl, double dt_max, double* dt_out)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (n < 0) return fail(&s->msg, DIMGPU_E_INVALID_ARG, "negative step count");
+    int rc = dimgpu_collect(s, nullptr, 0, nullptr);
+    if (rc) return rc;
+    for (int done = 0; done < n;) {
+        const int chunk = (n - done < kHistCap) ? (n - done) : kHistCap;
+        rc = dimgpu_enqueue_steps(s, chunk, cfl, dt_max);
+        if (rc) return rc;
+        rc = dimgpu_collect(s, dt_out ? dt_out + done : nullptr, chunk, nullptr);
+        if (rc) return rc;
+        done += chunk;
+    }
+    return DIMGPU_OK;
+}
+
+int dimgpu_totals(dimgpu_session* s, double* out)
+{
+    if (!s || !out) return fail(s ? &s->msg : nullptr, DIMGPU_E_INVALID_ARG, "null argument");
+    double volume = 1.0;
+    for (int a = 0; a < s->desc.dim; ++a) volume *= s->desc.dx[a];
+    int nb = 1;
+    cudaError_t e = cudaSuccess;
+    DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                e = launch_totals<NM, D>(s->g, s->buf[s->cur], volume, s->partial, kTotalsBlocks, &nb, s->stream));
+    const int NV = s->desc.nmat + 1 + s->desc.dim + 1;
+    std::vector<double> h((size_t)nb * NV);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), s->partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_totals");
+    for (int v = 0; v < NV; ++v) {
+        double acc = 0.0;
+        for (int b = 0; b < nb; ++b) acc += h[(size_t)b * NV + v];
+        out[v] = acc;
+    }
+    return DIMGPU_OK;
+}
+
+int dimgpu_set_stream(dimgpu_session* s, void* cuda_stream)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    cudaStreamSynchronize(s->stream);
+    s->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : s->own_stream;
+    return DIMGPU_OK;
+}
+
+int dimgpu_set_tile(dimgpu_session* s, int dir, int T, int W)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (dir < 0 || dir > 2 || T < 8 || W < 1 || T * W > 256 || (T * W) % 32 != 0)
+        return fail(&s->msg, DIMGPU_E_INVALID_ARG, "tile must satisfy 8 <= T, T*W <= 256, T*W a multiple of 32");
+    s->tile[dir] = {T, W};
+    return DIMGPU_OK;
+}
+
+int dimgpu_profile(dimgpu_session* s, int enable)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    prof_drain(s);
+    std::memset(s->prof, 0, sizeof s->prof);
+    s->profiling = enable != 0;
+    return DIMGPU_OK;
+}
+
+int dimgpu_profile_read(dimgpu_session* s, double* out8)
+{
+    if (!s || !out8) return fail(s ? &s->msg : nullptr, DIMGPU_E_INVALID_ARG, "null argument");
+    prof_drain(s);
+    std::memcpy(out8, s->prof, sizeof s->prof);
+    return DIMGPU_OK;
+}
+
+// One cached session per calling thread, rebuilt when the descriptor changes.
+int dimgpu_advance_one_step(const dimgpu_desc* desc, const double* soa_in, double* soa_out, double cfl,
+                            double dt_max, double* dt_out, dimgpu_phase_times* times)
+{
+    thread_local dimgpu_session* cached = nullptr;
+    thread_local dimgpu_desc cached_desc;
+    int rc = validate_desc(desc, nullptr);
+    if (rc) return rc;
+    if (!cached || std::memcmp(&cached_desc, desc, sizeof(dimgpu_desc)) != 0) {
+        dimgpu_destroy(cached);
+        cached = nullptr;
+        rc = dimgpu_create(desc, &cached);
+        if (rc) return rc;
+        cached_desc = *desc;
+    }
+    const size_t count = (size_t)cached->V * (size_t)cached->ncell;
+    if ((rc = dimgpu_upload(cached, soa_in, count))) { g_err = cached->msg; return rc; }
+    if ((rc = dimgpu_step(cached, cfl, dt_max, dt_out, times))) { g_err = cached->msg; return rc; }
+    if ((rc = dimgpu_download(cached, soa_out, count))) { g_err = cached->msg; return rc; }
+    return DIMGPU_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,7 @@
+// Kernel instantiations for 3 material(s), all dimensions (compiled in
+// parallel with the other material counts).
+#include "dim_kernels.cuh"
+
+namespace dimgpu {
+DIMGPU_INSTANTIATE(3)
+}  // namespace dimgpu

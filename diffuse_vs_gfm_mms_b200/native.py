@@ -1,0 +1,71 @@
+"""Loader of the in-tree CUDA library libdimgpu.so (built by build.py).
+
+There is no CPU fallback: importing the solver without the library, or
+calling it on a machine without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from . import abi
+
+LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "libdimgpu.so")
+
+# name -> (argtypes, restype)
+_D = C.POINTER(abi.Desc)
+_S = C.c_void_p
+_DP = abi.DPTR
+SIGNATURES = {
+    "dimgpu_components": ([_D], C.c_int),
+    "dimgpu_create": ([_D, C.POINTER(C.c_void_p)], C.c_int),
+    "dimgpu_destroy": ([_S], C.c_int),
+    "dimgpu_last_error": ([_S], C.c_char_p),
+    "dimgpu_upload": ([_S, _DP, C.c_size_t], C.c_int),
+    "dimgpu_download": ([_S, _DP, C.c_size_t], C.c_int),
+    "dimgpu_step": ([_S, C.c_double, C.c_double, _DP, C.POINTER(abi.PhaseTimes)], C.c_int),
+    "dimgpu_steps": ([_S, C.c_int, C.c_double, C.c_double, _DP], C.c_int),
+    "dimgpu_enqueue_steps": ([_S, C.c_int, C.c_double, C.c_double], C.c_int),
+    "dimgpu_collect": ([_S, _DP, C.c_int, C.POINTER(C.c_int)], C.c_int),
+    "dimgpu_compute_dt_cfl": ([_S, C.c_double, C.c_double, _DP], C.c_int),
+    "dimgpu_sweep_direction": ([_S, C.c_int, C.c_double], C.c_int),
+    "dimgpu_apply_boundary_conditions": ([_S], C.c_int),
+    "dimgpu_totals": ([_S, _DP], C.c_int),
+    "dimgpu_set_stream": ([_S, C.c_void_p], C.c_int),
+    "dimgpu_set_tile": ([_S, C.c_int, C.c_int, C.c_int], C.c_int),
+    "dimgpu_profile": ([_S, C.c_int], C.c_int),
+    "dimgpu_profile_read": ([_S, _DP], C.c_int),
+    "dimgpu_advance_one_step": ([_D, _DP, _DP, C.c_double, C.c_double, _DP,
+                                 C.POINTER(abi.PhaseTimes)], C.c_int),
+}
+
+_lib = None
+
+
+class DimGpuError(RuntimeError):
+    """A non-zero dimgpu status; .status holds the code (abi.E_*)."""
+
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{abi.STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+def lib() -> C.CDLL:
+    """The loaded library (loads it on first use; raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run python -m diffuse_vs_gfm_mms_b200.build")
+        L = C.CDLL(LIB_PATH)
+        for name, (argtypes, restype) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = argtypes
+            f.restype = restype
+        _lib = L
+    return _lib
+
+
+def check(rc: int, session=None) -> None:
+    if rc != 0:
+        msg = lib().dimgpu_last_error(session)
+        raise DimGpuError(rc, msg.decode() if msg else "")

@@ -162,6 +162,16 @@ int dimgpu_step(dimgpu_session* s, double cfl, double dt_max, double* dt_out,
  * (src/app/solver/run_dim.hpp:88-111). */
 int dimgpu_steps(dimgpu_session* s, int n, double cfl, double dt_max, double* dt_out);
 
+/* Asynchronous form of dimgpu_steps: enqueue n steps on the session's stream
+ * and return without waiting.  The dts stay on the device (at most 4096
+ * enqueued steps between collections). */
+int dimgpu_enqueue_steps(dimgpu_session* s, int n, double cfl, double dt_max);
+
+/* Wait for the enqueued steps, copy their dts into dt_out (room for
+ * `capacity` doubles; may be NULL), report how many in *count (may be NULL)
+ * and return the first error any of them raised. */
+int dimgpu_collect(dimgpu_session* s, double* dt_out, int capacity, int* count);
+
 /* CFL time step of the resident state.  Replaces dim::compute_dt_cfl
  * (src/dim/solver/cfl.hpp:16-66) and, for DIMGPU_TIME_UNSPLIT sessions,
  * dim::compute_dt_cfl_unsplit (src/dim/solver/cfl.hpp:70-119). */
@@ -176,11 +186,30 @@ int dimgpu_sweep_direction(dimgpu_session* s, int dir, double dt);
  * dim::apply_boundary_conditions (src/dim/solver/advance/boundary.hpp:165-226). */
 int dimgpu_apply_boundary_conditions(dimgpu_session* s);
 
-/* Mass per material, momentum per axis and total energy summed over all
- * cells and multiplied by the cell volume; out receives nmat + dim + 1
- * doubles.  Device counterpart of compute_dim_conservation_totals
- * (src/app/io/conservation_report.hpp:188-218). */
+/* Conservation totals of the resident state: out receives nmat + dim + 2
+ * doubles {material_mass[nmat], mass, momentum[dim], energy}, each the sum
+ * over cells of the conserved variable times the cell volume.  Device
+ * counterpart of compute_dim_conservation_totals
+ * (src/app/io/conservation_report.hpp:188-218); the summation order differs,
+ * so compare with a relative tolerance. */
 int dimgpu_totals(dimgpu_session* s, double* out);
+
+/* Run the session's work on a caller-owned CUDA stream (a cudaStream_t cast
+ * to void*; NULL restores the session's own stream).  The caller keeps the
+ * stream alive while the session uses it. */
+int dimgpu_set_stream(dimgpu_session* s, void* cuda_stream);
+
+/* Tile shape of the sweep kernel along axis `dir`: T cells per line segment
+ * (T - 6 of them are written, 6 are stencil halo) times W lines per CTA,
+ * 8 <= T, T * W <= 256.  Results do not depend on the tile shape. */
+int dimgpu_set_tile(dimgpu_session* s, int dir, int T, int W);
+
+/* Kernel timing: when enabled, every kernel the session launches is
+ * bracketed by CUDA events on its stream.  dimgpu_profile_read synchronises
+ * and writes {total_ms, launches} for the kinds sweep, cfl, boundary, other
+ * (8 doubles), accumulated since profiling was last enabled. */
+int dimgpu_profile(dimgpu_session* s, int enable);
+int dimgpu_profile_read(dimgpu_session* s, double* out8);
 
 /* Stateless drop-in for one call of dim::advance_one_step
  * (src/dim/solver/advance_step.hpp:150-270): host SoA in, host SoA out.
