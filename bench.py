@@ -1,0 +1,362 @@
+"""Benchmark of the B200 DIM step (one JSON line on rank 0).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c0]
+    python bench.py --impl reference ...      # the reference's own CPU code
+
+A step is one DIM time step (CFL reduction, one split sweep per axis, a
+boundary fill after each) over the whole grid of the workload:
+
+  c1  2D shock-bubble, 1024x512, two materials (the default: the metric's
+      configuration that fits one GPU);
+  c2  3D bubble cloud, 512^3, two materials;
+  c0  1D two-material Riemann tube, 1000 cells.
+
+value  = cell updates per second with the state resident in HBM (CUDA events
+         on the session's stream, one event pair per step; the L2 is flushed
+         between steps when the state fits in it);
+e2e    = the same metric through the C-ABI with host buffers: every step
+         uploads the state from pinned host memory, steps, and downloads the
+         new state and dt (dim::advance_one_step's by-value contract);
+roofline = the sweep kernel's algorithmic bytes (read + write of the V-double
+         state per cell) over its average event-timed duration, against the
+         measured HBM copy bandwidth.
+Multi-GPU: the single-grid step does not shard; N GPUs run N replicas
+("scaling": "weak") and value is the sum over ranks / the slowest rank.
+"""
+from __future__ import annotations
+
+import argparse
+import glob
+import json
+import os
+import re
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "DIM cell-updates/s"
+UNIT = "cell-updates/s"
+
+WORKLOADS = {
+    "c1": ("2D shock-bubble 1024x512, 2 materials, Mach 1.22, CFL 0.8", 0.8),
+    "c2": ("3D bubble cloud 512^3, 64 air bubbles in stiffened water, CFL 0.6", 0.6),
+    "c0": ("1D two-material Riemann tube 1000 cells, CFL 0.8", 0.8),
+}
+
+
+def make_workload(name: str, scale: int = 1):
+    from diffuse_vs_gfm_mms_b200 import workloads as W
+    if name == "c1":
+        return W.shock_bubble_2d(N=(1024 // scale, 512 // scale))
+    if name == "c2":
+        n = 512 // scale
+        return W.bubble_cloud_3d(N=(n, n, n), nbubbles=64)
+    if name == "c0":
+        return W.riemann(seed=0, N=(1000,))
+    raise SystemExit(f"unknown workload {name}")
+
+
+def reference_sample(name: str):
+    """The bounded CPU sample of a workload: same spacing and physics, fewer lines."""
+    from diffuse_vs_gfm_mms_b200 import workloads as W
+    if name == "c1":
+        d, U = W.shock_bubble_2d(N=(1024, 512))
+        # a strip of 64 rows x 1024 columns around the bubble's centre line
+        V = d.nvar
+        U3 = U.reshape(V, 512, 1024)[:, 224:288, :]
+        d2 = d.copy()
+        d2.N[1] = 64
+        return d2, np.ascontiguousarray(U3.reshape(V, -1)), "1024x64 strip of the 1024x512 grid (rows 224-287)"
+    if name == "c2":
+        d, U = W.bubble_cloud_3d(N=(64, 64, 64), nbubbles=64)
+        d.dx[0] = d.dx[1] = d.dx[2] = 1.0 / 512
+        return d, U, "64^3 block of the 512^3 case (same spacing, 64 bubbles)"
+    d, U = W.riemann(seed=0, N=(1000,))
+    return d, U, "the whole 1000-cell tube"
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            j = json.load(f)
+        return float(j["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic(workload: str):
+    """dram bytes (read + write) per sweep launch from the committed ncu
+    summaries: a line `traffic_bytes_per_launch <workload> <bytes>`."""
+    for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
+        with open(path) as f:
+            for line in f:
+                m = re.match(r"\s*traffic_bytes_per_launch\s+(\S+)\s+([0-9.eE+]+)", line)
+                if m and m.group(1) == workload:
+                    return float(m.group(2)), os.path.relpath(path, ROOT)
+    return None, None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = os.path.join("/tmp", f"dimgpu_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax = float(parts[2])
+                except ValueError:
+                    continue
+                for nm, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
+                "samples": len(sm), "reasons": sorted(reasons)}
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_rate(workload: str, steps: int, warmup: int):
+    """The reference's OpenMP code (oracle/_ref) on the host cores, on the
+    bounded sample of the workload; falls back to the C restatement."""
+    nthreads = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(nthreads))
+    os.environ.setdefault("OMP_PROC_BIND", "close")
+    os.environ.setdefault("OMP_PLACES", "cores")
+    os.environ.setdefault("OMP_SCHEDULE", "guided,1")
+    os.environ.setdefault("OMP_DYNAMIC", "FALSE")
+    from oracle import oracle as O
+    kind = "reference" if O.reference_available() else "port"
+    chk = O.reference() if kind == "reference" else O.port()
+    chk.set_threads(nthreads)
+    d, U, sample = reference_sample(workload)
+    cfl = WORKLOADS[workload][1]
+    if warmup:
+        U, _ = chk.advance(d, U, cfl, 1e300, warmup)
+    t0 = time.perf_counter()
+    chk.advance(d, U, cfl, 1e300, steps)
+    el = time.perf_counter() - t0
+    rate = d.ncell * steps / el
+    return {"value": rate, "unit": UNIT, "cores": chk.max_threads(), "kind": kind,
+            "sample": f"{sample}; {steps} steps after {warmup} warm-up", "seconds": el}
+
+
+def run_reference(args):
+    world, rank, _ = dist_init()
+    if rank != 0:
+        return
+    steps = max(1, args.steps)
+    cb = cpu_reference_rate(args.workload, steps, min(args.warmup, 1))
+    line = {
+        "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": cb["seconds"] / steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": {"workload": WORKLOADS[args.workload][0], "parallelism": "cpu-openmp"},
+        "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+        "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    from diffuse_vs_gfm_mms_b200.dim import Session
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+
+    d, U = make_workload(args.workload, args.scale)
+    cfl = WORKLOADS[args.workload][1]
+    ncell, V = d.ncell, d.nvar
+    state_bytes = ncell * V * 8
+    l2_bytes = 126 * 1024 * 1024
+    flush_l2 = 2 * state_bytes < 2 * l2_bytes  # both ping-pong buffers could stay resident
+    stream = torch.cuda.Stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda") if flush_l2 else None
+
+    s = Session(d, U)
+    s.set_stream(stream.cuda_stream)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # warm-up
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            s.enqueue_steps(1, cfl, 1e300)
+        s.collect()
+
+    # ---- device-resident timing
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    barrier()
+    s.profile(True)
+    with ClockSampler(local) as clk, torch.cuda.stream(stream):
+        for k in range(args.steps):
+            if flush is not None:
+                flush.zero_()
+            evs[k][0].record(stream)
+            s.enqueue_steps(1, cfl, 1e300)
+            evs[k][1].record(stream)
+        stream.synchronize()
+    barrier()
+    step_ms = [a.elapsed_time(b) for a, b in evs]
+    prof = s.profile_read()
+    s.profile(False)
+    dts = s.collect()
+    total_ms = float(sum(step_ms))
+    clocks = clk.summary()
+
+    # ---- end to end through the C-ABI with pinned host buffers
+    pin_in = torch.empty(V * ncell, dtype=torch.float64, pin_memory=True)
+    pin_out = torch.empty(V * ncell, dtype=torch.float64, pin_memory=True)
+    pin_in.numpy()[:] = s.download().reshape(-1)
+    e2e_evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(args.steps)]
+    with torch.cuda.stream(stream):
+        for k in range(max(1, args.warmup)):
+            s.upload(pin_in.numpy())
+            s.enqueue_steps(1, cfl, 1e300)
+            s.collect()
+            s.download(pin_out.numpy().reshape(V, ncell))
+        barrier()
+        for k in range(args.steps):
+            if flush is not None:
+                flush.zero_()
+            e2e_evs[k][0].record(stream)
+            s.upload(pin_in.numpy())
+            s.enqueue_steps(1, cfl, 1e300)
+            s.download(pin_out.numpy().reshape(V, ncell))
+            s.collect()
+            e2e_evs[k][1].record(stream)
+            pin_in, pin_out = pin_out, pin_in
+        stream.synchronize()
+    barrier()
+    e2e_ms = float(sum(a.elapsed_time(b) for a, b in e2e_evs))
+
+    # ---- max over ranks
+    if world > 1:
+        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms, e2e_ms = float(t[0]), float(t[1])
+
+    s.close()
+    if rank != 0:
+        if world > 1:
+            dist.destroy_process_group()
+        return
+
+    value = world * ncell * args.steps / (total_ms * 1e-3)
+    e2e_value = world * ncell * args.steps / (e2e_ms * 1e-3)
+    sweep = prof["sweep"]
+    avg_sweep_s = sweep["ms"] / max(sweep["launches"], 1) * 1e-3
+    alg_bytes = 2 * V * 8 * ncell  # read + write of the state, per sweep launch
+    achieved = alg_bytes / avg_sweep_s / 1e9
+    peak, peak_src = measured_peaks()
+    traffic, traffic_src = ncu_traffic(args.workload)
+    launches = sum(v["launches"] for v in prof.values())
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {
+            "workload": WORKLOADS[args.workload][0], "cells": ncell, "components": V,
+            "parallelism": f"replicas x{world}" if world > 1 else "single-gpu",
+            "l2": "flushed between steps" if flush_l2 else "state larger than L2",
+            "tiles": "default", "last_dt": float(dts[-1]) if len(dts) else None,
+        },
+        "roofline": {
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "kernel": "sweep_kernel",
+            "note": f"algorithmic {alg_bytes} B per sweep launch (2*V*8*cells); avg sweep "
+                    f"{avg_sweep_s * 1e3:.4f} ms over {sweep['launches']} launches; peak {peak_src}"
+                    + (f"; traffic from {traffic_src}" if traffic_src else ""),
+        },
+        "phase_ms": {k: v["ms"] for k, v in prof.items()},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * ncell * 8,
+                "d2h_bytes_per_step": V * ncell * 8 + 8},
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+    if world == 1 and not args.no_cpu:
+        cb = cpu_reference_rate(args.workload, steps=2 if args.workload != "c0" else 20, warmup=0)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--scale", type=int, default=1, help="divide the grid sides (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
