@@ -5,6 +5,8 @@
 
 #include <cuda_runtime.h>
 
+#include <string>
+
 #include "dim_physics.h"
 
 namespace dimgpu {
@@ -57,5 +59,8 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
                           int max_blocks, int* nblocks, cudaStream_t s);
 
 int sweep_smem_doubles(int nmat, int dim);
+
+// Message returned by dimgpu_last_error(NULL) on the calling thread.
+void set_sessionless_error(const std::string& msg);
 
 }  // namespace dimgpu

@@ -87,6 +87,8 @@ cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_m
 
 int sweep_smem_doubles(int nmat, int dim) { return (2 * nmat + dim) + (2 * nmat + dim + 1); }
 
+void set_sessionless_error(const std::string& msg) { g_err = msg; }
+
 }  // namespace dimgpu
 
 struct dimgpu_session {

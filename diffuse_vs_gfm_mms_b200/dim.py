@@ -150,6 +150,21 @@ class Session:
         return {k: {"ms": float(out[2 * i]), "launches": int(out[2 * i + 1])} for i, k in enumerate(kinds)}
 
 
+def compute_dt_cfl_noalloc(desc: Desc, device_ptr: int, cfl: float, dt_max: float,
+                           stream_handle: int | None = None) -> float:
+    """CFL dt of a state the caller keeps in its own device memory
+    (device_ptr: address of the SoA array), without any device allocation.
+
+    For callers that manage all GPU memory themselves and cannot have the
+    library allocate mid-loop.  At most 4 194 304 cells; the library's one
+    static scratch array per GPU is shared by all calls, so overlapping calls
+    on the same device race."""
+    dt = C.c_double()
+    check(lib().dimgpu_compute_dt_cfl_noalloc(C.byref(desc), C.cast(C.c_void_p(device_ptr), abi.DPTR), cfl,
+                                              dt_max, C.byref(dt), C.c_void_p(stream_handle or 0)))
+    return dt.value
+
+
 def advance_one_step(U: np.ndarray, desc: Desc, cfl: float, dt_max: float,
                      timings: bool = False) -> StepResult:
     """Stateless drop-in for dim::advance_one_step: host SoA in, StepResult out."""

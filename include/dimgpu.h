@@ -211,6 +211,26 @@ int dimgpu_set_tile(dimgpu_session* s, int dir, int T, int W);
 int dimgpu_profile(dimgpu_session* s, int enable);
 int dimgpu_profile_read(dimgpu_session* s, double* out8);
 
+/* CFL time step of a state that the caller keeps in its own device memory,
+ * computed without allocating anything.  No counterpart in the reference: it
+ * serves callers that own all device memory themselves (a serving process
+ * holding the HBM budget for resident solves, a solver handing out buffers
+ * from its own pool) and so cannot let a library call cudaMalloc — which may
+ * fail for lack of memory and which synchronises the device — mid time loop.
+ *
+ * d_state: device pointer to the SoA state (layout above); the result is
+ * written to the host double *dt_out; work runs on `cuda_stream` (a
+ * cudaStream_t cast to void*, NULL for the default stream) and the call
+ * returns once dt is on the host.  Same value as dimgpu_compute_dt_cfl.
+ *
+ * Limits: at most 4 194 304 cells (larger grids return DIMGPU_E_INVALID_ARG
+ * before any device work).  The scratch is one 128 KB array per GPU, static
+ * to the library and kept until the process exits; the first call on a
+ * device looks up its address and should come before any stream capture.
+ * All calls share that array, so calls that overlap on the GPU race. */
+int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const double* d_state, double cfl,
+                                  double dt_max, double* dt_out, void* cuda_stream);
+
 /* Stateless drop-in for one call of dim::advance_one_step
  * (src/dim/solver/advance_step.hpp:150-270): host SoA in, host SoA out.
  * Uses a cached session per descriptor shape; the copies are part of the call. */
