@@ -48,6 +48,9 @@ LAMBDA_MODELS = {"kapila": 0, "": 0, "allaire": 1, "equal_velocity": 2}
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
 
+SCHEDULE_FUSED = 0
+SCHEDULE_STAGED = 1
+
 TIME_SPLIT = 0
 TIME_UNSPLIT = 1
 

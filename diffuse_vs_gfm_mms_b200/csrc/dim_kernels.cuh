@@ -139,7 +139,7 @@ __host__ __device__ constexpr int kSweepSmemVars(int nm, int d) { return kStateV
 // Stage k+1 of a cell reads stage-k results of its two neighbours from shared
 // memory, so every stage is separated by one __syncthreads.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
+__global__ void __launch_bounds__(256, 2) sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                     Grid g, Mats M, int T, int W, int ntile, int ngx,
                                                     const double* __restrict__ dtp, int* __restrict__ err)
 {
@@ -259,6 +259,270 @@ __global__ void __launch_bounds__(256) sweep_kernel(const double* __restrict__ i
         stage_e<NM, D>(M, U, A, first ? nullptr : &lo, last ? nullptr : &fd, first, last, dt, dx, Un);
         store_cell<NM, D>(out, g.ncell, cell, Un);
     }
+}
+
+// ---- the staged sweep ---------------------------------------------------------------
+//
+// The same five stages as sweep_kernel, one kernel per stage over a chunk of
+// whole lines, with the per-cell results handed between stages through a
+// scratch area in global memory instead of shared memory.  Each kernel is
+// small (fits the instruction cache), needs no CTA barrier and computes every
+// cell exactly once (no tile halo); the price is the scratch traffic, about
+// ten times the state traffic of the fused kernel, which the step's
+// arithmetic intensity leaves room for.
+//
+// Work item t of a chunk of nl lines x n cells: for the x sweep t = line*n +
+// i (cells of a line are consecutive threads), for y / z t = i*nl + line
+// (consecutive threads are consecutive x columns).  Scratch record var v of
+// item t sits at buf[v * cap + t]; the neighbour along the line is t +- s
+// with s = 1 (x) or nl (y, z).
+struct LineSet {
+    long long L0;  // first line of the chunk
+    int nl;        // lines in the chunk
+    int n;         // cells per line
+};
+
+template<int NM, int D>
+struct StagedBufs {
+    double* P;    // cons_to_prim(U)             kPrimVars
+    double* ck;   // alpha-RHS sound speeds       NM
+    double* Pe;   // enforce(P)                   kPrimVars
+    double* Ph;   // half-step primitive          kPrimVars
+    double* LS;   // left face state              kStateVars
+    double* RS;   // right face state             kStateVars
+    double* PLS;  // cons_to_prim(LS)             kPrimVars
+    double* PRS;  // cons_to_prim(RS)             kPrimVars
+    double* F;    // face i|i+1: flux, s*, alpha flux   2*NM + D + 2
+    long long cap;
+};
+
+__host__ __device__ constexpr int kFaceVars(int nm, int d) { return 2 * nm + d + 2; }
+// P, Pe, Ph, PLS, PRS + ck + LS, RS + the face record
+__host__ __device__ constexpr int kStagedVars(int nm, int d)
+{
+    return 5 * kPrimVars(nm, d) + nm + 2 * kStateVars(nm, d) + kFaceVars(nm, d);
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_put(double* b, long long cap, long long t, const Prim<NM, D>& P)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = P.rho[k];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = P.alpha[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) b[(v++) * cap + t] = P.vel[d];
+    b[v * cap + t] = P.p;
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_get(const double* b, long long cap, long long t, Prim<NM, D>& P)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) P.rho[k] = b[(v++) * cap + t];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) P.alpha[k] = b[(v++) * cap + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) P.vel[d] = b[(v++) * cap + t];
+    P.p = b[v * cap + t];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_put(double* b, long long cap, long long t, const State<NM, D>& U)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = U.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) b[(v++) * cap + t] = U.mom[d];
+    b[(v++) * cap + t] = U.E;
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) b[(v++) * cap + t] = U.a[k];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_get(const double* b, long long cap, long long t, State<NM, D>& U)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) U.m[k] = b[(v++) * cap + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) U.mom[d] = b[(v++) * cap + t];
+    U.E = b[(v++) * cap + t];
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) U.a[k] = b[(v++) * cap + t];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_put(double* b, long long cap, long long t, const FaceD<NM, D>& f)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = f.F.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) b[(v++) * cap + t] = f.F.mom[d];
+    b[(v++) * cap + t] = f.F.E;
+    b[(v++) * cap + t] = f.fv;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = f.af[k];
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_get(const double* b, long long cap, long long t, FaceD<NM, D>& f)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) f.F.m[k] = b[(v++) * cap + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) f.F.mom[d] = b[(v++) * cap + t];
+    f.F.E = b[(v++) * cap + t];
+    f.fv = b[(v++) * cap + t];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) f.af[k] = b[(v++) * cap + t];
+}
+
+// Item t of a chunk: its cell index along the line, its cell in the grid and
+// the scratch stride between neighbours along the line.
+template<int DIR>
+struct StagedItem {
+    int gi;
+    long long cell;
+    long long s;
+    __device__ __forceinline__ StagedItem(const Grid& g, const LineSet& ls, long long t)
+    {
+        long long lrel;
+        if (DIR == 0) { lrel = t / ls.n; gi = (int)(t % ls.n); s = 1; }
+        else { gi = (int)(t / ls.nl); lrel = t % ls.nl; s = ls.nl; }
+        const long long L = ls.L0 + lrel;
+        long long base;
+        if (DIR == 0) base = L * g.N[0];
+        else if (DIR == 1) base = (L % g.N[0]) + (L / g.N[0]) * g.stride[2];
+        else base = (L % g.N[0]) + (L / g.N[0]) * g.stride[1];
+        cell = base + (long long)gi * g.stride[DIR];
+    }
+};
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) staged_a(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                                StagedBufs<NM, D> b)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    State<NM, D> U;
+    load_cell<NM, D>(in, g.ncell, it.cell, U);
+    CellA<NM, D> A;
+    stage_a<NM, D>(M, U, A);
+    g_put<NM, D>(b.P, b.cap, t, A.P);
+    g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) staged_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                                StagedBufs<NM, D> b, const double* __restrict__ dtp)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
+    CellA<NM, D> A;
+    g_get<NM, D>(b.Pe, b.cap, t, A.Pe);
+    Prim<NM, D> Ph;
+    if (end) {
+        Ph = A.Pe;
+    }
+    else {
+        State<NM, D> U;
+        load_cell<NM, D>(in, g.ncell, it.cell, U);
+#pragma unroll
+        for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
+        Prim<NM, D> lo, hi;
+        g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
+        g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+        State<NM, D> Uh;
+        stage_b<NM, D>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Uh, Ph);
+    }
+    g_put<NM, D>(b.Ph, b.cap, t, Ph);
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) staged_c(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                                StagedBufs<NM, D> b)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
+    State<NM, D> LS, RS;
+    Prim<NM, D> PLS, PRS;
+    if (end) {
+        load_cell<NM, D>(in, g.ncell, it.cell, LS);
+        RS = LS;
+        g_get<NM, D>(b.P, b.cap, t, PLS);
+        PRS = PLS;
+    }
+    else {
+        CellA<NM, D> A;  // only read for end cells
+        State<NM, D> U;
+        Prim<NM, D> Ph, lo, hi;
+        g_get<NM, D>(b.Ph, b.cap, t, Ph);
+        g_get<NM, D>(b.Ph, b.cap, t - it.s, lo);
+        g_get<NM, D>(b.Ph, b.cap, t + it.s, hi);
+        stage_c<NM, D>(M, U, A, Ph, lo, hi, false, LS, RS, PLS, PRS);
+    }
+    g_put<NM, D>(b.LS, b.cap, t, LS);
+    g_put<NM, D>(b.RS, b.cap, t, RS);
+    g_put<NM, D>(b.PLS, b.cap, t, PLS);
+    g_put<NM, D>(b.PRS, b.cap, t, PRS);
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) staged_d(Grid g, Mats M, LineSet ls, StagedBufs<NM, D> b,
+                                                int* __restrict__ err)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    if (it.gi >= ls.n - 1) return;  // face i|i+1 exists for i <= n-2
+    State<NM, D> UL, UR;
+    Prim<NM, D> PL, PR;
+    g_get<NM, D>(b.RS, b.cap, t, UL);
+    g_get<NM, D>(b.PRS, b.cap, t, PL);
+    g_get<NM, D>(b.LS, b.cap, t + it.s, UR);
+    g_get<NM, D>(b.PLS, b.cap, t + it.s, PR);
+    FaceD<NM, D> f;
+    if (!stage_d<NM, D>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    g_put<NM, D>(b.F, b.cap, t, f);
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) staged_e(const double* __restrict__ in, double* __restrict__ out, Grid g,
+                                                Mats M, LineSet ls, StagedBufs<NM, D> b,
+                                                const double* __restrict__ dtp)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    const bool first = it.gi == 0, last = it.gi == n - 1;
+    State<NM, D> U;
+    load_cell<NM, D>(in, g.ncell, it.cell, U);
+    CellA<NM, D> A;
+    g_get<NM, D>(b.P, b.cap, t, A.P);
+#pragma unroll
+    for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
+    FaceD<NM, D> lo, hi;
+    if (!first) g_get<NM, D>(b.F, b.cap, t - it.s, lo);
+    if (!last) g_get<NM, D>(b.F, b.cap, t, hi);
+    State<NM, D> Un;
+    stage_e<NM, D>(M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, *dtp, g.dx[DIR], Un);
+    store_cell<NM, D>(out, g.ncell, it.cell, Un);
 }
 
 // ---- CFL ------------------------------------------------------------------------
@@ -558,6 +822,60 @@ cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const
     return cudaErrorInvalidValue;
 }
 
+// Staged schedule: chunks of whole lines, at most `cap` cells each; scratch
+// holds kStagedVars(NM, D) * cap doubles.
+template<int NM, int D, int DIR>
+cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, double* out, const double* dt, int* err,
+                              double* scratch, long long cap, cudaStream_t s)
+{
+    const int n = g.N[DIR];
+    const long long nlines = g.ncell / n;
+    long long per = cap / n;
+    if (per < 1) return cudaErrorInvalidValue;
+    StagedBufs<NM, D> b;
+    b.cap = cap;
+    double* p = scratch;
+    b.P = p; p += kPrimVars(NM, D) * cap;
+    b.ck = p; p += NM * cap;
+    b.Pe = p; p += kPrimVars(NM, D) * cap;
+    b.Ph = p; p += kPrimVars(NM, D) * cap;
+    b.LS = p; p += kStateVars(NM, D) * cap;
+    b.RS = p; p += kStateVars(NM, D) * cap;
+    b.PLS = p; p += kPrimVars(NM, D) * cap;
+    b.PRS = p; p += kPrimVars(NM, D) * cap;
+    b.F = p;
+    for (long long L0 = 0; L0 < nlines; L0 += per) {
+        LineSet ls;
+        ls.L0 = L0;
+        ls.nl = (int)((nlines - L0 < per) ? (nlines - L0) : per);
+        ls.n = n;
+        const long long items = (long long)ls.nl * n;
+        const unsigned blocks = (unsigned)((items + 255) / 256);
+        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b);
+        staged_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        staged_c<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b);
+        staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
+        staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template<int NM, int D>
+cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const double* in, double* out,
+                                const double* dt, int* err, double* scratch, long long cap, cudaStream_t s)
+{
+    if (dir == 0) return launch_staged_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, s);
+    if constexpr (D >= 2) {
+        if (dir == 1) return launch_staged_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, s);
+    }
+    if constexpr (D >= 3) {
+        if (dir == 2) return launch_staged_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
                        double* blockmin, int max_blocks, int* nblocks, cudaStream_t s)
@@ -626,6 +944,8 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
 #define DIMGPU_INSTANTIATE_D(NM, D)                                                                          \
     template cudaError_t launch_sweep<NM, D>(const Grid&, const Mats&, int, Tile, const double*, double*,    \
                                              const double*, int*, cudaStream_t);                             \
+    template cudaError_t launch_sweep_staged<NM, D>(const Grid&, const Mats&, int, const double*, double*,   \
+                                                    const double*, int*, double*, long long, cudaStream_t);  \
     template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
                                            int, int*, cudaStream_t);                                         \
     template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \

@@ -36,6 +36,15 @@ template<int NM, int D>
 cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const double* in, double* out,
                          const double* dt, int* err, cudaStream_t s);
 
+// The staged schedule of the same sweep: stages A..E as separate kernels
+// over chunks of whole lines of at most `cap` cells, intermediates in
+// `scratch` (staged_scratch_doubles(nmat, dim) * cap doubles).
+template<int NM, int D>
+cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const double* in, double* out,
+                                const double* dt, int* err, double* scratch, long long cap, cudaStream_t s);
+
+int staged_scratch_doubles(int nmat, int dim);
+
 // Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,

@@ -22,10 +22,16 @@
 #include <cfloat>
 #include <cmath>
 
+// DHD: small helpers, inlined.  DNI: the large routines every sweep calls at
+// many sites (pressure recovery, cons_to_prim, prim_to_cons, repair_state,
+// the generic sound speed), kept as single out-of-line copies on the device
+// so the sweep kernel's code fits the instruction cache.
 #ifdef __CUDACC__
 #define DHD __host__ __device__ __forceinline__
+#define DNI __host__ __device__ __noinline__
 #else
 #define DHD inline
+#define DNI inline
 #endif
 
 namespace dimgpu {
@@ -181,7 +187,7 @@ struct MixtureBisection {
 };
 
 template<int NM>
-DHD double pressure_from_internal_energy(const Mats& M, double rho_total, double e,
+DNI double pressure_from_internal_energy(const Mats& M, double rho_total, double e,
                                          const double* alpha, const double* rho)
 {
     rho_total = clamp_min(rho_total);
@@ -264,11 +270,26 @@ DHD double pressure_from_internal_energy(const Mats& M, double rho_total, double
 
     if (!flo_ok || !fhi_ok) return clamp_min(fallback_pressure);
 
+    // Inside the loop lo <= mid <= hi, all finite and positive, so
+    // clamp_min(mid) == max(mid, 1e-10); below P_fin the certain decisions
+    // are two compares and two selects.
+    const bool fast_loop = fast && clamp_min(hi) < P_fin;
     for (int n = 0; n < 80; ++n) {
         const double mid = 0.5 * (lo + hi);
-        s = status(mid);
-        if (s > 0) { hi = mid; continue; }
-        if (s < 0) { lo = mid; continue; }
+        if (fast_loop) {
+            const double pc = dmax(mid, 1e-10);
+            const bool up = pc > P_hi, dn = pc < P_lo;
+            if (up || dn) {
+                hi = up ? mid : hi;
+                lo = dn ? mid : lo;
+                continue;
+            }
+        }
+        else {
+            s = status(mid);
+            if (s > 0) { hi = mid; continue; }
+            if (s < 0) { lo = mid; continue; }
+        }
         const double fmid = R.literal(M, mid);
         if (!fin(fmid)) return clamp_min(fallback_pressure);
         if (fabs(fmid) <= thresh) return clamp_min(mid);
@@ -297,7 +318,7 @@ DHD double mixture_sound_speed(const Mats& M, double rho_total, double p, const 
 
 // MixtureEOS::generic_mixture_sound_speed, src/dim/eos.hpp:223-275
 template<int NM>
-DHD double generic_mixture_sound_speed(const Mats& M, double rho_total, double p,
+DNI double generic_mixture_sound_speed(const Mats& M, double rho_total, double p,
                                        const double* alpha, const double* rho)
 {
     if (M.lambda_model == 0) return mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
@@ -375,7 +396,7 @@ DHD double total_density(const State<NM, D>& U)
 
 // cons_to_prim, primitives.hpp:111-162
 template<int NM, int D>
-DHD void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+DNI void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
 {
     full_alpha<NM, D>(U, P.alpha);
     sanitise_alpha<NM>(P.alpha, 1e-12);
@@ -402,7 +423,7 @@ DHD void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
 // prim_to_cons, primitives.hpp:165-212 (internal_energy_from_pressure,
 // src/dim/eos.hpp:146-166, inlined)
 template<int NM, int D>
-DHD void prim_to_cons(const Mats& M, Prim<NM, D> P, State<NM, D>& U)
+DNI void prim_to_cons(const Mats& M, Prim<NM, D> P, State<NM, D>& U)
 {
     sanitise_alpha<NM>(P.alpha, 1e-12);
     double rho_total = 0.0;
@@ -497,7 +518,7 @@ DHD void alpha_rhs_coefficients(const Mats& M, const Prim<NM, D>& P, const doubl
 
 // repair_state, primitives.hpp:325-457.
 template<int NM, int D>
-DHD void repair_state(const Mats& M, State<NM, D>& U)
+DNI void repair_state(const Mats& M, State<NM, D>& U)
 {
     const double mass_floor = 1e-12, p_floor = 1e-12, inactive_alpha_floor = 1e-10;
 #pragma unroll

@@ -87,6 +87,12 @@ cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_m
 
 int sweep_smem_doubles(int nmat, int dim) { return (2 * nmat + dim) + (2 * nmat + dim + 1); }
 
+int staged_scratch_doubles(int nmat, int dim)
+{
+    const int pv = 2 * nmat + dim + 1, v = 2 * nmat + dim, fv = 2 * nmat + dim + 2;
+    return 5 * pv + nmat + 2 * v + fv;
+}
+
 void set_sessionless_error(const std::string& msg) { g_err = msg; }
 
 }  // namespace dimgpu
@@ -107,6 +113,9 @@ struct dimgpu_session {
     cudaStream_t own_stream = nullptr;
     cudaStream_t stream = nullptr;
     Tile tile[3] = {{128, 1}, {64, 4}, {64, 4}};
+    int schedule[3] = {DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED};
+    double* staged = nullptr;  // scratch of the staged schedule (allocated on first use)
+    long long staged_cap = 0;
     std::string msg;
     // profiling
     bool profiling = false;
@@ -235,10 +244,34 @@ cudaError_t run_cfl(dimgpu_session* s, double cfl, double dt_max, double* hist)
     return launch_cfl_finalize(s->blockmin, nb, dt_max, s->dt, hist, s->err, s->stream);
 }
 
+constexpr long long kStagedChunkCells = 1LL << 24;
+
+cudaError_t ensure_staged_scratch(dimgpu_session* s)
+{
+    if (s->staged) return cudaSuccess;
+    long long cap = s->ncell < kStagedChunkCells ? s->ncell : kStagedChunkCells;
+    for (int a = 0; a < 3; ++a)
+        if (s->g.N[a] > cap) cap = s->g.N[a];
+    const size_t bytes = sizeof(double) * (size_t)staged_scratch_doubles(s->desc.nmat, s->desc.dim) * (size_t)cap;
+    cudaError_t e = cudaMalloc(&s->staged, bytes);
+    if (e == cudaSuccess) s->staged_cap = cap;
+    return e;
+}
+
 cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out)
 {
     cudaError_t e = cudaSuccess;
+    if (s->schedule[dir] == DIMGPU_SCHEDULE_STAGED) {
+        e = ensure_staged_scratch(s);
+        if (e != cudaSuccess) return e;
+    }
     ProfScope p(s, kSweep);
+    if (s->schedule[dir] == DIMGPU_SCHEDULE_STAGED) {
+        DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                    e = launch_sweep_staged<NM, D>(s->g, s->M, dir, in, out, s->dt, s->err, s->staged,
+                                                   s->staged_cap, s->stream));
+        return e;
+    }
     DISPATCH_ND(s->desc.nmat, s->desc.dim,
                 e = launch_sweep<NM, D>(s->g, s->M, dir, s->tile[dir], in, out, s->dt, s->err, s->stream));
     return e;
@@ -370,6 +403,7 @@ int dimgpu_destroy(dimgpu_session* s)
     cudaFree(s->hist);
     cudaFree(s->partial);
     cudaFree(s->err);
+    cudaFree(s->staged);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     delete s;
     return DIMGPU_OK;
@@ -553,6 +587,15 @@ int dimgpu_set_tile(dimgpu_session* s, int dir, int T, int W)
     if (dir < 0 || dir > 2 || T < 8 || W < 1 || T * W > 256 || (T * W) % 32 != 0)
         return fail(&s->msg, DIMGPU_E_INVALID_ARG, "tile must satisfy 8 <= T, T*W <= 256, T*W a multiple of 32");
     s->tile[dir] = {T, W};
+    return DIMGPU_OK;
+}
+
+int dimgpu_set_schedule(dimgpu_session* s, int dir, int schedule)
+{
+    if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");
+    if (dir < 0 || dir > 2 || (schedule != DIMGPU_SCHEDULE_FUSED && schedule != DIMGPU_SCHEDULE_STAGED))
+        return fail(&s->msg, DIMGPU_E_INVALID_ARG, "schedule must be DIMGPU_SCHEDULE_FUSED or _STAGED");
+    s->schedule[dir] = schedule;
     return DIMGPU_OK;
 }
 

@@ -140,6 +140,10 @@ class Session:
     def set_tile(self, direction: int, T: int, W: int) -> None:
         self._check(lib().dimgpu_set_tile(self._h, direction, T, W))
 
+    def set_schedule(self, direction: int, schedule: int) -> None:
+        """abi.SCHEDULE_FUSED (one tiled kernel) or abi.SCHEDULE_STAGED (a kernel per stage)."""
+        self._check(lib().dimgpu_set_schedule(self._h, direction, schedule))
+
     def profile(self, enable: bool) -> None:
         self._check(lib().dimgpu_profile(self._h, 1 if enable else 0))
 

@@ -33,6 +33,7 @@ SIGNATURES = {
     "dimgpu_totals": ([_S, _DP], C.c_int),
     "dimgpu_set_stream": ([_S, C.c_void_p], C.c_int),
     "dimgpu_set_tile": ([_S, C.c_int, C.c_int, C.c_int], C.c_int),
+    "dimgpu_set_schedule": ([_S, C.c_int, C.c_int], C.c_int),
     "dimgpu_profile": ([_S, C.c_int], C.c_int),
     "dimgpu_profile_read": ([_S, _DP], C.c_int),
     "dimgpu_compute_dt_cfl_noalloc": ([_D, _DP, C.c_double, C.c_double, _DP, C.c_void_p], C.c_int),

@@ -84,6 +84,12 @@ enum {
     DIMGPU_PRECISION_MIXED = 1  /* FP32 reconstruction + HLLC, FP64 state/EoS/dt      */
 };
 
+/* Sweep schedules (results are identical; speed differs by grid shape). */
+enum {
+    DIMGPU_SCHEDULE_FUSED = 0,   /* one kernel: all stages in a shared-memory tile      */
+    DIMGPU_SCHEDULE_STAGED = 1   /* one kernel per stage, intermediates in HBM scratch   */
+};
+
 /* Config::time_update (src/io/config.hpp:112). */
 enum {
     DIMGPU_TIME_SPLIT = 0,
@@ -203,6 +209,11 @@ int dimgpu_set_stream(dimgpu_session* s, void* cuda_stream);
  * (T - 6 of them are written, 6 are stencil halo) times W lines per CTA,
  * 8 <= T, T * W <= 256.  Results do not depend on the tile shape. */
 int dimgpu_set_tile(dimgpu_session* s, int dir, int T, int W);
+
+/* Sweep schedule along axis `dir` (DIMGPU_SCHEDULE_*).  The staged schedule
+ * allocates its scratch (about 60 doubles per cell, at most 2^24 cells per
+ * chunk) on first use. */
+int dimgpu_set_schedule(dimgpu_session* s, int dir, int schedule);
 
 /* Kernel timing: when enabled, every kernel the session launches is
  * bracketed by CUDA events on its stream.  dimgpu_profile_read synchronises

@@ -135,6 +135,32 @@ def test_tile_shape_does_not_change_results():
     assert ndiff(outs[0], outs[1]) == 0 and ndiff(outs[0], outs[2]) == 0
 
 
+@pytest.mark.parametrize("N", [(33, 17, 9), (130, 3), (5, 70), (300,), (2, 9)])
+def test_staged_schedule_matches_oracle(port, N):
+    """The staged schedule (a kernel per stage, HBM scratch) on every axis."""
+    d, U = W.riemann(seed=5, N=N, axis=len(N) - 1)
+    with Session(d, U) as s:
+        for direction in range(d.dim):
+            s.set_schedule(direction, abi.SCHEDULE_STAGED)
+        dts = s.steps(6, 0.5, 1e300)
+        out = s.download()
+    ref, rdts = port.advance(d, U, 0.5, 1e300, 6)
+    assert ndiff(out, ref) == 0 and bitwise_equal(dts, rdts)
+
+
+def test_schedules_agree_on_c1():
+    d, U = W.shock_bubble_2d(N=(512, 256))
+    outs = []
+    for sched in ((abi.SCHEDULE_FUSED,) * 2, (abi.SCHEDULE_STAGED,) * 2,
+                  (abi.SCHEDULE_STAGED, abi.SCHEDULE_FUSED)):
+        with Session(d, U) as s:
+            for direction, k in enumerate(sched):
+                s.set_schedule(direction, k)
+            s.steps(5, 0.8, 1e300)
+            outs.append(s.download())
+    assert ndiff(outs[0], outs[1]) == 0 and ndiff(outs[0], outs[2]) == 0
+
+
 def test_large_3d_lines_match_oracle(port):
     """256^3 cloud, one x sweep, then y, then z: sampled lines against the
     oracle's solve_line (a size-independent check of the full-size grid)."""
