@@ -46,6 +46,9 @@ WORKLOADS = {
     "c1": ("2D shock-bubble 1024x512, 2 materials, Mach 1.22, CFL 0.8", 0.8),
     "c2": ("3D bubble cloud 512^3, 64 air bubbles in stiffened water, CFL 0.6", 0.6),
     "c0": ("1D two-material Riemann tube 1000 cells, CFL 0.8", 0.8),
+    "c4": ("Poisson stream of DIM requests: 40% 1D N in [256,8192], 60% 2D sides in [128,2048], "
+           "steps in [100,2000], 150 GB budget", 0.6),
+    "c3": ("256 independent 2D instances, sides log-uniform in [64,1024], Riemann or bubble, CFL 0.6", 0.6),
 }
 
 
@@ -340,6 +343,135 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_batch(args):
+    """Config 3: the batched form against sequential plain solves.
+
+    value = instances solved per second by one batched run of every instance
+    for `c3_steps` steps (persistent-grid launches replayed from a CUDA
+    graph); the sequential baseline runs a sample of the same instances one
+    at a time through the plain session path on the same GPU."""
+    import torch
+
+    from diffuse_vs_gfm_mms_b200.batch import Batch
+    from diffuse_vs_gfm_mms_b200.dim import Session
+    from diffuse_vs_gfm_mms_b200 import workloads as W
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    cfl = WORKLOADS["c3"][1]
+    steps = args.c3_steps
+    inst = W.batch_instances(args.c3_instances, seed=rank)
+    cells = sum(d.ncell for d, _ in inst)
+    stream = torch.cuda.Stream()
+
+    # warm-up: kernels loaded, graphs captured on a small batch
+    with Batch(2, 2) as w:
+        w.set_stream(stream.cuda_stream)
+        for d, U in W.batch_instances(4, seed=99, side_range=(64, 96)):
+            w.add(d, U, 3 * 8, cfl)
+        w.run(3 * 8)
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    with Batch(2, 2) as b, ClockSampler(local) as clk:
+        b.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ev[0].record(stream)
+        ids = [b.add(d, U, steps, cfl) for d, U in inst]
+        ev[1].record(stream)
+        b.run(steps)
+        ev[2].record(stream)
+        outs = [b.download(i, with_dts=False)[0] for i in ids[:: max(1, len(ids) // 8)]]
+        ev[3].record(stream)
+        stream.synchronize()
+    run_ms = ev[1].elapsed_time(ev[2])
+    e2e_ms = ev[0].elapsed_time(ev[3])
+    clocks = clk.summary()
+
+    # sequential plain solves on a sample of the same instances
+    sample = inst[:: max(1, len(inst) // args.c3_sequential)]
+    seq_ms = 0.0
+    for d, U in sample:
+        with Session(d, U) as s:
+            s.set_stream(stream.cuda_stream)
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s.enqueue_steps(steps, cfl, 1e300)
+            z.record(stream)
+            s.collect()
+            seq_ms += a.elapsed_time(z)
+    sample_cells = sum(d.ncell for d, _ in sample)
+    seq_cell_rate = sample_cells * steps / (seq_ms * 1e-3)
+    # the whole instance set run one at a time, estimated from the sample's
+    # per-cell cost (the sample's mean size differs from the set's)
+    seq_rate = len(inst) / (cells * steps / seq_cell_rate)
+    value = len(inst) / (run_ms * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": "DIM batched solves/s", "value": world * value, "unit": "solves/s", "n_gpus": world,
+            "steps": steps, "warmup": 1, "ms_per_step": run_ms / steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOADS["c3"][0], "instances": len(inst), "cells": cells,
+                       "steps_per_instance": steps, "l2": "state larger than L2"},
+            "batched_cell_updates_per_s": cells * steps / (run_ms * 1e-3),
+            "sequential_plain": {"solves_per_s": seq_rate, "cell_updates_per_s": seq_cell_rate,
+                                 "sample": f"{len(sample)} of the {len(inst)} instances run one at a time; "
+                                           "solves/s of the whole set at the sample's cost per cell update"},
+            "speedup_vs_sequential_plain": value / seq_rate,
+            "e2e": {"value": world * len(inst) / (e2e_ms * 1e-3), "unit": "solves/s",
+                    "h2d_bytes_per_step": sum(U.nbytes for _, U in inst) / steps,
+                    "d2h_bytes_per_step": sum(o.nbytes for o in outs) / steps},
+            "clocks": clocks,
+        }
+        print(json.dumps(line), flush=True)
+
+
+def run_serving(args):
+    """Config 4: the continuous-batching server against the sequential plain
+    path on the same request stream, at each arrival rate of --c4-rates."""
+    import torch
+
+    from diffuse_vs_gfm_mms_b200 import serve
+
+    world, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    stream = torch.cuda.Stream()
+    # warm-up: kernels loaded and the batch graphs captured
+    warm = serve.make_requests(4, 0.0, seed=1000, steps_range=(16, 16), n1d_range=(256, 256),
+                               side2d_range=(128, 128))
+    with serve.Server(stream_handle=stream.cuda_stream) as srv:
+        srv.serve(warm)
+    serve.sequential(warm[:1], stream_handle=stream.cuda_stream)
+    rows = []
+    with ClockSampler(local) as clk:
+        for rate in args.c4_rates:
+            reqs = serve.make_requests(args.c4_requests, rate, seed=7 + rank)
+            with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8,
+                              stream_handle=stream.cuda_stream) as srv:
+                st = srv.serve(reqs)
+            sq = serve.sequential(reqs, stream_handle=stream.cuda_stream)
+            p50, p99 = st.latency_percentiles()
+            q50, q99 = sq.latency_percentiles()
+            rows.append({"rate_per_s": rate, "served": {"solves_per_s": st.solves_per_s, "p50_s": p50, "p99_s": p99,
+                                                        "peak_slots": st.peak_slots,
+                                                        "peak_gb": st.peak_bytes / 1e9},
+                         "sequential_plain": {"solves_per_s": sq.solves_per_s, "p50_s": q50, "p99_s": q99}})
+    if rank == 0:
+        best = max(rows, key=lambda r: r["served"]["solves_per_s"])
+        line = {
+            "metric": "DIM served solves/s", "value": world * best["served"]["solves_per_s"], "unit": "solves/s",
+            "n_gpus": world, "steps": args.c4_requests, "warmup": 1, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOADS["c4"][0],
+                       "requests_per_rate": args.c4_requests, "rates": args.c4_rates,
+                       "sample": f"{args.c4_requests} requests per rate of the 10,000-request stream"},
+            "rates": rows,
+            "speedup_vs_sequential_plain": best["served"]["solves_per_s"] / best["sequential_plain"]["solves_per_s"],
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -349,11 +481,21 @@ def main():
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--scale", type=int, default=1, help="divide the grid sides (profiling runs)")
+    ap.add_argument("--c3-steps", type=int, default=500)
+    ap.add_argument("--c3-instances", type=int, default=256)
+    ap.add_argument("--c3-sequential", type=int, default=16, help="instances in the sequential sample")
+    ap.add_argument("--c4-requests", type=int, default=32)
+    ap.add_argument("--c4-rates", type=float, nargs="+", default=[1.0, 4.0])
+    ap.add_argument("--c4-slots", type=int, default=128)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "c3":
+        run_batch(args)
+    elif args.workload == "c4":
+        run_serving(args)
     else:
         run_ours(args)
 

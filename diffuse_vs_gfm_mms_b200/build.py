@@ -24,8 +24,9 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
          "-ccbin", "g++", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
-SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "dimgpu_api.cu", "dimgpu_noalloc.cu"]
-HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h"]
+SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "dimgpu_api.cu", "dimgpu_noalloc.cu",
+           "dimgpu_batch.cu"]
+HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h", "dim_batch.cuh"]
 
 
 def _mtime(p):

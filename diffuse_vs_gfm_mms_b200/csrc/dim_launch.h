@@ -67,6 +67,40 @@ template<int NM, int D>
 cudaError_t launch_totals(const Grid& g, const double* state, double volume, double* partial,
                           int max_blocks, int* nblocks, cudaStream_t s);
 
+// ---- batched form (dim_batch.cuh) ----
+// One entry per instance of a batch, in device memory.
+struct BInst {
+    Grid g;
+    Mats M;
+    double* st[2];      // ping-pong state buffers (SoA, ncell stride)
+    double* dtlog;      // dt of every step run, capacity = steps requested
+    long long soff;     // first scratch item of this instance
+    int steps_left;     // steps still to run
+    int steps_done;     // steps run so far
+    int run;            // runs in the current step (set by the finalize kernel)
+    int pad;
+    double cfl, dt_max;
+    double dt;          // dt of the current step
+};
+
+// Device tables and scratch of one batched step.
+struct BatchLaunch {
+    BInst* tab;
+    const long long* cell_prefix;  // work blocks of 256 cells per instance
+    const long long* bc_prefix;    // work blocks of 256 boundary cells per instance
+    int ninst;
+    double* blockmin;
+    double* scratch;
+    long long cap;                 // scratch items
+    int* err;
+    int grid;                      // persistent grid size
+};
+
+// One time step of every running instance: per-instance CFL, the staged
+// sweeps and boundary fills, with a persistent grid of L.grid CTAs.
+template<int NM, int D>
+cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s);
+
 int sweep_smem_doubles(int nmat, int dim);
 
 // Message returned by dimgpu_last_error(NULL) on the calling thread.

@@ -1,0 +1,486 @@
+// dimgpu_batch.cu — the batched form of the DIM step (include/dimgpu.h,
+// dimgpu_batch_*): many independent grids of one material count and
+// dimension, each with its own size, materials, boundaries, cfl, dt_max and
+// step budget, advanced together by one set of persistent-grid launches per
+// step (dim_batch.cuh) and replayed from a captured CUDA graph.
+//
+// Membership (instances added, finished, removed) lives in device tables;
+// the launch geometry does not depend on it, so one captured graph of G steps
+// serves every membership as long as the scratch and tables are not
+// reallocated.  Each instance's arithmetic is exactly the single-grid step's,
+// so an instance's result is the same alone, in any batch, and against the
+// oracle.
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "dim_launch.h"
+#include "dimgpu.h"
+
+using namespace dimgpu;
+
+namespace {
+
+constexpr int kGraphSteps = 8;  // steps per captured graph (even: parity returns for any dim)
+
+struct HostInst {
+    int id;
+    dimgpu_desc desc;
+    BInst dev;            // what is uploaded into the device table
+    long long ncell;
+    long long nbc;        // boundary cells
+    int steps_total;
+    int steps_left;       // host mirror (exact: every run advances min(n, left))
+};
+
+long long boundary_cells(const dimgpu_desc& d)
+{
+    long long total = 0;
+    for (int a = 0; a < d.dim; ++a) {
+        if (d.N[a] <= 1) continue;
+        long long c = 1;
+        for (int b = 0; b < d.dim; ++b) {
+            if (b == a) continue;
+            c *= (b < a && d.N[b] != 1) ? (long long)(d.N[b] - 2) : (long long)d.N[b];
+        }
+        total += 2 * c;
+    }
+    return total;
+}
+
+}  // namespace
+
+struct dimgpu_batch {
+    int nmat = 0, dim = 0;
+    std::vector<HostInst> inst;
+    int next_id = 1;
+    int parity = 0;
+    bool dirty = true;      // tables must be rebuilt before the next step
+    // device
+    BInst* tab = nullptr;
+    long long* cell_prefix = nullptr;
+    long long* bc_prefix = nullptr;
+    double* blockmin = nullptr;
+    double* scratch = nullptr;
+    int* err = nullptr;
+    long long tab_cap = 0, blockmin_cap = 0, scratch_cap = 0;
+    int grid = 148 * 4;
+    cudaStream_t stream = nullptr;
+    cudaStream_t own_stream = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by start parity
+    std::string msg;
+};
+
+namespace {
+
+int bfail(dimgpu_batch* b, int code, const std::string& m)
+{
+    if (b) b->msg = m;
+    set_sessionless_error(m);
+    return code;
+}
+
+int bcuda(dimgpu_batch* b, cudaError_t e, const char* what)
+{
+    if (e == cudaErrorMemoryAllocation) return bfail(b, DIMGPU_E_OOM, std::string(what) + ": out of device memory");
+    return bfail(b, DIMGPU_E_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void drop_graphs(dimgpu_batch* b)
+{
+    for (auto& g : b->graph) {
+        if (g) cudaGraphExecDestroy(g);
+        g = nullptr;
+    }
+}
+
+template<class T>
+cudaError_t grow(T** p, long long* cap, long long need)
+{
+    if (need <= *cap && *p) return cudaSuccess;
+    long long n = std::max<long long>(need, *cap * 3 / 2);
+    n = std::max<long long>(n, 16);
+    cudaFree(*p);
+    *p = nullptr;
+    cudaError_t e = cudaMalloc(p, sizeof(T) * (size_t)n);
+    if (e == cudaSuccess) *cap = n;
+    else *cap = 0;
+    return e;
+}
+
+// Pull the device-side counters of the current members into the host mirror.
+cudaError_t pull_counters(dimgpu_batch* b)
+{
+    if (b->inst.empty() || !b->tab || b->dirty) return cudaSuccess;
+    std::vector<BInst> dev(b->inst.size());
+    cudaError_t e = cudaMemcpyAsync(dev.data(), b->tab, sizeof(BInst) * dev.size(), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return e;
+    for (size_t i = 0; i < dev.size(); ++i) {
+        b->inst[i].dev.steps_left = dev[i].steps_left;
+        b->inst[i].dev.steps_done = dev[i].steps_done;
+        b->inst[i].dev.run = dev[i].run;
+        b->inst[i].dev.dt = dev[i].dt;
+    }
+    return cudaSuccess;
+}
+
+// Rebuild the device tables (and grow the scratch) for the current members.
+// Tables are padded to a capacity C (entries past the members have no work
+// and no steps), and every launch is given C, so a captured graph stays valid
+// across membership changes until a table or the scratch has to grow.
+cudaError_t rebuild(dimgpu_batch* b)
+{
+    const int n = (int)b->inst.size();
+    long long items = 0, cells_blocks = 0;
+    for (int i = 0; i < n; ++i) {
+        b->inst[i].dev.soff = items;
+        items += b->inst[i].ncell;
+        cells_blocks += (b->inst[i].ncell + 255) / 256;
+    }
+    const int nrec = staged_scratch_doubles(b->nmat, b->dim);
+    const void* before[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
+    cudaError_t e = grow(&b->scratch, &b->scratch_cap, std::max<long long>(items, 1) * nrec);
+    if (e == cudaSuccess) e = grow(&b->blockmin, &b->blockmin_cap, std::max<long long>(cells_blocks, 1));
+    if (e == cudaSuccess && (n > b->tab_cap || !b->tab)) {
+        const long long cap = std::max<long long>(std::max<long long>(16, n), b->tab_cap * 2);
+        cudaFree(b->tab);
+        cudaFree(b->cell_prefix);
+        cudaFree(b->bc_prefix);
+        b->tab = nullptr;
+        b->cell_prefix = b->bc_prefix = nullptr;
+        e = cudaMalloc(&b->tab, sizeof(BInst) * (size_t)cap);
+        if (e == cudaSuccess) e = cudaMalloc(&b->cell_prefix, sizeof(long long) * (size_t)(cap + 1));
+        if (e == cudaSuccess) e = cudaMalloc(&b->bc_prefix, sizeof(long long) * (size_t)(cap + 1));
+        b->tab_cap = e == cudaSuccess ? cap : 0;
+    }
+    if (e != cudaSuccess) return e;
+    const void* after[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
+    if (std::memcmp(before, after, sizeof before) != 0) drop_graphs(b);
+    const long long C = b->tab_cap;
+    std::vector<BInst> dev((size_t)C);
+    std::memset(dev.data(), 0, sizeof(BInst) * (size_t)C);
+    std::vector<long long> cp((size_t)C + 1, 0), bp((size_t)C + 1, 0);
+    for (long long i = 0; i < C; ++i) {
+        long long cb = 0, bb = 0;
+        if (i < n) {
+            dev[i] = b->inst[i].dev;
+            cb = (b->inst[i].ncell + 255) / 256;
+            bb = (b->inst[i].nbc + 255) / 256;
+        }
+        cp[i + 1] = cp[i] + cb;
+        bp[i + 1] = bp[i] + bb;
+    }
+    e = cudaMemcpyAsync(b->tab, dev.data(), sizeof(BInst) * (size_t)C, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->cell_prefix, cp.data(), sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
+                            b->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(b->bc_prefix, bp.data(), sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
+                            b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return e;
+    b->dirty = false;
+    return cudaSuccess;
+}
+
+BatchLaunch launch_args(dimgpu_batch* b)
+{
+    BatchLaunch L;
+    L.tab = b->tab;
+    L.cell_prefix = b->cell_prefix;
+    L.bc_prefix = b->bc_prefix;
+    L.ninst = (int)b->tab_cap;
+    L.blockmin = b->blockmin;
+    L.scratch = b->scratch;
+    L.cap = b->scratch_cap / staged_scratch_doubles(b->nmat, b->dim);
+    L.err = b->err;
+    L.grid = b->grid;
+    return L;
+}
+
+cudaError_t one_step(dimgpu_batch* b, const BatchLaunch& L, int parity)
+{
+    cudaError_t e = cudaErrorInvalidValue;
+    switch (b->nmat * 10 + b->dim) {
+#define BATCH_CASE(NM, D) \
+        case NM * 10 + D: e = batch_step<NM, D>(L, parity, b->stream); break;
+        BATCH_CASE(1, 1) BATCH_CASE(1, 2) BATCH_CASE(1, 3)
+        BATCH_CASE(2, 1) BATCH_CASE(2, 2) BATCH_CASE(2, 3)
+        BATCH_CASE(3, 1) BATCH_CASE(3, 2) BATCH_CASE(3, 3)
+        BATCH_CASE(4, 1) BATCH_CASE(4, 2) BATCH_CASE(4, 3)
+#undef BATCH_CASE
+        default: break;
+    }
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dimgpu_batch_create(int nmat, int dim, dimgpu_batch** out)
+{
+    if (!out) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    if (nmat < 1 || nmat > DIMGPU_MAX_MATERIALS) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "nmat must be 1..4");
+    if (dim < 1 || dim > 3) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "dim must be 1, 2 or 3");
+    auto* b = new dimgpu_batch();
+    b->nmat = nmat;
+    b->dim = dim;
+    cudaError_t e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&b->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
+    int dev = 0, sms = 148;
+    if (e == cudaSuccess) e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) {
+        const int rc = bcuda(nullptr, e, "dimgpu_batch_create");
+        dimgpu_batch_destroy(b);
+        return rc;
+    }
+    b->grid = sms * 4;
+    b->own_stream = b->stream;
+    *out = b;
+    return DIMGPU_OK;
+}
+
+int dimgpu_batch_destroy(dimgpu_batch* b)
+{
+    if (!b) return DIMGPU_OK;
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    drop_graphs(b);
+    for (auto& h : b->inst) {
+        cudaFree(h.dev.st[0]);
+        cudaFree(h.dev.st[1]);
+        cudaFree(h.dev.dtlog);
+    }
+    cudaFree(b->tab);
+    cudaFree(b->cell_prefix);
+    cudaFree(b->bc_prefix);
+    cudaFree(b->blockmin);
+    cudaFree(b->scratch);
+    cudaFree(b->err);
+    if (b->own_stream) cudaStreamDestroy(b->own_stream);
+    else if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return DIMGPU_OK;
+}
+
+const char* dimgpu_batch_last_error(const dimgpu_batch* b) { return b ? b->msg.c_str() : ""; }
+
+int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, int steps, double cfl, double dt_max,
+                     int* id)
+{
+    if (!b || !d || !soa || !id) return bfail(b, DIMGPU_E_INVALID_ARG, "null argument");
+    if (d->nmat != b->nmat || d->dim != b->dim)
+        return bfail(b, DIMGPU_E_INVALID_ARG, "instance nmat / dim differ from the batch's");
+    if (d->time_update != DIMGPU_TIME_SPLIT) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs split steps only");
+    if (d->precision != DIMGPU_PRECISION_FP64) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs FP64 only");
+    if (steps < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative step count");
+    if (!(cfl > 0.0) || !(dt_max > 0.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "cfl and dt_max must be positive");
+    long long ncell = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (a < d->dim && d->N[a] < 1) return bfail(b, DIMGPU_E_INVALID_ARG, "grid size must be positive");
+        if (a >= d->dim && d->N[a] != 1) return bfail(b, DIMGPU_E_INVALID_ARG, "unused axes must have N = 1");
+        if (a < d->dim && !(d->dx[a] > 0.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "grid spacing must be positive");
+        if (a < d->dim && (d->N[a] == 2 || d->N[a] == 3))
+            return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch needs N = 1 or N >= 4 on every axis");
+        ncell *= d->N[a];
+    }
+    for (int k = 0; k < d->nmat; ++k) {
+        if (d->mat[k].kind != DIMGPU_EOS_IDEAL_GAS && d->mat[k].kind != DIMGPU_EOS_STIFFENED_GAS)
+            return bfail(b, DIMGPU_E_UNSUPPORTED_EOS, "only ideal_gas and stiffened_gas run on the GPU");
+        if (!(d->mat[k].gamma > 1.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "gamma must be > 1");
+    }
+    if (d->lambda_model < 0 || d->lambda_model > 2) return bfail(b, DIMGPU_E_INVALID_ARG, "unknown lambda model");
+
+    cudaError_t e = pull_counters(b);
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_add");
+    HostInst h{};
+    h.id = b->next_id++;
+    h.desc = *d;
+    h.ncell = ncell;
+    h.nbc = boundary_cells(*d);
+    h.steps_total = steps;
+    h.steps_left = steps;
+    std::memset(&h.dev, 0, sizeof h.dev);
+    BInst& I = h.dev;
+    int kind[kMaxMat];
+    double gam[kMaxMat], pinf[kMaxMat];
+    for (int k = 0; k < d->nmat; ++k) {
+        kind[k] = d->mat[k].kind;
+        gam[k] = d->mat[k].gamma;
+        pinf[k] = d->mat[k].p_inf;
+    }
+    fill_mats(I.M, d->nmat, kind, gam, pinf, d->lambda_model, d->alpha_source_floor);
+    for (int a = 0; a < 3; ++a) {
+        I.g.N[a] = d->N[a];
+        I.g.dx[a] = d->dx[a];
+        I.g.bc_lo[a] = d->bc_lo[a];
+        I.g.bc_hi[a] = d->bc_hi[a];
+    }
+    I.g.ncell = ncell;
+    I.g.stride[0] = 1;
+    I.g.stride[1] = d->N[0];
+    I.g.stride[2] = (long long)d->N[0] * d->N[1];
+    I.steps_left = steps;
+    I.cfl = cfl;
+    I.dt_max = dt_max;
+    const size_t bytes = sizeof(double) * (size_t)(2 * d->nmat + d->dim) * (size_t)ncell;
+    e = cudaMalloc(&I.st[0], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&I.st[1], bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&I.dtlog, sizeof(double) * (size_t)std::max(steps, 1));
+    if (e == cudaSuccess) e = cudaMemcpyAsync(I.st[b->parity], soa, bytes, cudaMemcpyHostToDevice, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) {
+        cudaFree(I.st[0]);
+        cudaFree(I.st[1]);
+        cudaFree(I.dtlog);
+        return bcuda(b, e, "dimgpu_batch_add");
+    }
+    b->inst.push_back(h);
+    b->dirty = true;
+    *id = h.id;
+    return DIMGPU_OK;
+}
+
+int dimgpu_batch_remove(dimgpu_batch* b, int id)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    cudaError_t e = pull_counters(b);
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_remove");
+    for (size_t i = 0; i < b->inst.size(); ++i) {
+        if (b->inst[i].id != id) continue;
+        cudaStreamSynchronize(b->stream);
+        cudaFree(b->inst[i].dev.st[0]);
+        cudaFree(b->inst[i].dev.st[1]);
+        cudaFree(b->inst[i].dev.dtlog);
+        b->inst.erase(b->inst.begin() + (long)i);
+        b->dirty = true;
+        return DIMGPU_OK;
+    }
+    return bfail(b, DIMGPU_E_INVALID_ARG, "no instance with this id");
+}
+
+// Advance every instance with steps left by up to n steps.
+int dimgpu_batch_run(dimgpu_batch* b, int n)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    if (n < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative step count");
+    if (b->inst.empty() || n == 0) return DIMGPU_OK;
+    cudaError_t e = cudaSuccess;
+    if (b->dirty) {
+        e = pull_counters(b);
+        if (e == cudaSuccess) e = rebuild(b);
+        if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
+    }
+    const BatchLaunch L = launch_args(b);
+    const bool odd = (b->dim % 2) == 1;
+    int done = 0;
+    while (done < n && e == cudaSuccess) {
+        if (n - done >= kGraphSteps) {
+            cudaGraphExec_t& g = b->graph[b->parity];
+            if (!g) {
+                cudaGraph_t graph;
+                e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+                int par = b->parity;
+                for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
+                    e = one_step(b, L, par);
+                    if (odd) par = 1 - par;
+                }
+                cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+                if (e == cudaSuccess) e = e2;
+                if (e == cudaSuccess) {
+                    e = cudaGraphInstantiate(&g, graph, 0);
+                    cudaGraphDestroy(graph);
+                }
+                if (e != cudaSuccess) break;
+            }
+            e = cudaGraphLaunch(g, b->stream);
+            done += kGraphSteps;  // kGraphSteps is even: the parity is unchanged
+        }
+        else {
+            e = one_step(b, L, b->parity);
+            if (odd) b->parity = 1 - b->parity;
+            done += 1;
+        }
+    }
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
+    for (auto& h : b->inst) h.steps_left = std::max(0, h.steps_left - n);
+    int flag = 0;
+    e = cudaMemcpyAsync(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
+    if (flag) {
+        cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
+        if (flag & kErrNonFinite)
+            return bfail(b, DIMGPU_E_NONFINITE, "dim::hllc_flux_normal: invalid density or pressure (non-finite)");
+        return bfail(b, DIMGPU_E_NONFINITE, "run_dim_case: non-positive timestep");
+    }
+    return DIMGPU_OK;
+}
+
+// Steps run and left for one instance (host-side mirror, no device sync).
+int dimgpu_batch_status(dimgpu_batch* b, int id, int* steps_done, int* steps_left)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    for (auto& h : b->inst) {
+        if (h.id != id) continue;
+        if (steps_done) *steps_done = h.steps_total - h.steps_left;
+        if (steps_left) *steps_left = h.steps_left;
+        return DIMGPU_OK;
+    }
+    return bfail(b, DIMGPU_E_INVALID_ARG, "no instance with this id");
+}
+
+// State of one instance (count = V * ncell doubles) and, if dts is not NULL,
+// the dt of each step it has run (room for steps_done doubles).
+int dimgpu_batch_download(dimgpu_batch* b, int id, double* soa, size_t count, double* dts)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    for (auto& h : b->inst) {
+        if (h.id != id) continue;
+        const size_t want = (size_t)(2 * h.desc.nmat + h.desc.dim) * (size_t)h.ncell;
+        if (soa && count != want) return bfail(b, DIMGPU_E_INVALID_ARG, "dimgpu_batch_download: size mismatch");
+        cudaError_t e = cudaSuccess;
+        if (soa)
+            e = cudaMemcpyAsync(soa, h.dev.st[b->parity], sizeof(double) * want, cudaMemcpyDeviceToHost, b->stream);
+        const int ndone = h.steps_total - h.steps_left;
+        if (e == cudaSuccess && dts && ndone > 0)
+            e = cudaMemcpyAsync(dts, h.dev.dtlog, sizeof(double) * (size_t)ndone, cudaMemcpyDeviceToHost, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+        return e == cudaSuccess ? DIMGPU_OK : bcuda(b, e, "dimgpu_batch_download");
+    }
+    return bfail(b, DIMGPU_E_INVALID_ARG, "no instance with this id");
+}
+
+// Persistent grid size (CTAs per launch); 0 restores SMs x 4.
+int dimgpu_batch_set_grid(dimgpu_batch* b, int ctas)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    if (ctas < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative grid");
+    int dev = 0, sms = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    b->grid = ctas ? ctas : sms * 4;
+    drop_graphs(b);
+    return DIMGPU_OK;
+}
+
+int dimgpu_batch_size(const dimgpu_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+// Run on a caller-owned stream (NULL: the batch's own).  Captured graphs are
+// kept: replaying them on another stream is valid.
+int dimgpu_batch_set_stream(dimgpu_batch* b, void* cuda_stream)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    cudaStreamSynchronize(b->stream);
+    if (!b->own_stream) b->own_stream = b->stream;
+    b->stream = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : b->own_stream;
+    return DIMGPU_OK;
+}
+
+}  // extern "C"

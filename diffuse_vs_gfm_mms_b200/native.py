@@ -37,6 +37,17 @@ SIGNATURES = {
     "dimgpu_profile": ([_S, C.c_int], C.c_int),
     "dimgpu_profile_read": ([_S, _DP], C.c_int),
     "dimgpu_compute_dt_cfl_noalloc": ([_D, _DP, C.c_double, C.c_double, _DP, C.c_void_p], C.c_int),
+    "dimgpu_batch_create": ([C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "dimgpu_batch_destroy": ([C.c_void_p], C.c_int),
+    "dimgpu_batch_last_error": ([C.c_void_p], C.c_char_p),
+    "dimgpu_batch_add": ([C.c_void_p, _D, _DP, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_int)], C.c_int),
+    "dimgpu_batch_remove": ([C.c_void_p, C.c_int], C.c_int),
+    "dimgpu_batch_run": ([C.c_void_p, C.c_int], C.c_int),
+    "dimgpu_batch_status": ([C.c_void_p, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)], C.c_int),
+    "dimgpu_batch_download": ([C.c_void_p, C.c_int, _DP, C.c_size_t, _DP], C.c_int),
+    "dimgpu_batch_set_grid": ([C.c_void_p, C.c_int], C.c_int),
+    "dimgpu_batch_size": ([C.c_void_p], C.c_int),
+    "dimgpu_batch_set_stream": ([C.c_void_p, C.c_void_p], C.c_int),
     "dimgpu_advance_one_step": ([_D, _DP, _DP, C.c_double, C.c_double, _DP,
                                  C.POINTER(abi.PhaseTimes)], C.c_int),
 }

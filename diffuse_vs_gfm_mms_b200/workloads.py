@@ -253,3 +253,21 @@ def random_states(desc: Desc, n: int, seed: int = 0, edge_fraction: float = 0.1)
         U[idx[3 * q:4 * q], nmat + dim] *= 1e-6                        # energy deficit
         U[idx[4 * q:], nmat:nmat + dim] *= 50.0                        # large momentum
     return U
+
+
+def batch_instances(n: int = 256, seed: int = 0, side_range=(64, 1024)):
+    """Config 3: n 2D instances, sides log-uniform in side_range per axis,
+    each a config-0 two-material Riemann problem (random axis and interface
+    position) or a single bubble, all with config-0 material draws."""
+    rng = np.random.default_rng(seed)
+    lo, hi = np.log(side_range[0]), np.log(side_range[1])
+    out = []
+    for k in range(n):
+        N = (int(round(np.exp(rng.uniform(lo, hi)))), int(round(np.exp(rng.uniform(lo, hi)))))
+        s = int(rng.integers(0, 2**31 - 1))
+        if rng.uniform() < 0.5:
+            axis = int(rng.integers(0, 2))
+            out.append(riemann(seed=s, N=N, axis=axis, position=float(rng.uniform(0.2, 0.8))))
+        else:
+            out.append(single_bubble_2d(N, seed=s))
+    return out

@@ -249,6 +249,47 @@ int dimgpu_advance_one_step(const dimgpu_desc* desc, const double* soa_in, doubl
                             double cfl, double dt_max, double* dt_out,
                             dimgpu_phase_times* times);
 
+/* ---- batched form ------------------------------------------------------
+ * Many independent grids (one material count and dimension per batch; each
+ * with its own N, dx, materials, boundaries, cfl, dt_max and step budget)
+ * advanced together: one set of persistent-grid launches per step for every
+ * instance, replayed from a captured CUDA graph.  Each instance's results are
+ * exactly those of a dimgpu_session run of the same grid.  Split steps, FP64,
+ * N = 1 or N >= 4 on every axis.  No counterpart in the reference, which
+ * runs one grid per process (src/app/solver/run_dim.hpp:20-178). */
+typedef struct dimgpu_batch dimgpu_batch;
+
+int dimgpu_batch_create(int nmat, int dim, dimgpu_batch** out);
+int dimgpu_batch_destroy(dimgpu_batch* b);
+const char* dimgpu_batch_last_error(const dimgpu_batch* b);
+
+/* Add an instance: copies `soa` (V * ncell doubles) to the device; the
+ * instance will run `steps` steps.  *id identifies it afterwards. */
+int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* desc, const double* soa, int steps,
+                     double cfl, double dt_max, int* id);
+
+/* Remove an instance and free its device memory. */
+int dimgpu_batch_remove(dimgpu_batch* b, int id);
+
+/* Advance every instance that has steps left by up to n steps. */
+int dimgpu_batch_run(dimgpu_batch* b, int n);
+
+/* Steps run / left of an instance (no device synchronisation). */
+int dimgpu_batch_status(dimgpu_batch* b, int id, int* steps_done, int* steps_left);
+
+/* State of an instance (count = V * ncell) and, if dts is not NULL, the dt
+ * of every step it has run. */
+int dimgpu_batch_download(dimgpu_batch* b, int id, double* soa, size_t count, double* dts);
+
+/* Persistent grid size in CTAs (0: 4 per SM). */
+int dimgpu_batch_set_grid(dimgpu_batch* b, int ctas);
+
+/* Number of instances in the batch. */
+int dimgpu_batch_size(const dimgpu_batch* b);
+
+/* Run the batch's work on a caller-owned CUDA stream (NULL: its own). */
+int dimgpu_batch_set_stream(dimgpu_batch* b, void* cuda_stream);
+
 #ifdef __cplusplus
 }
 #endif
