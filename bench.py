@@ -93,8 +93,9 @@ def measured_peaks():
 
 
 def ncu_traffic(workload: str):
-    """dram bytes (read + write) per sweep launch from the committed ncu
-    summaries: a line `traffic_bytes_per_launch <workload> <bytes>`."""
+    """dram bytes (read + write) per sweep (all kernels of one sweep) from the
+    committed ncu summaries: a line `traffic_bytes_per_launch <workload>
+    <bytes>` (workload `c1`, or `c1-mixed` for the mixed-precision form)."""
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as f:
             for line in f:
@@ -211,6 +212,7 @@ def run_ours(args):
     import torch
     import torch.distributed as dist
 
+    from diffuse_vs_gfm_mms_b200 import native
     from diffuse_vs_gfm_mms_b200.dim import Session
 
     world, rank, local = dist_init()
@@ -220,6 +222,9 @@ def run_ours(args):
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
     d, U = make_workload(args.workload, args.scale)
+    if args.precision == "mixed":
+        from diffuse_vs_gfm_mms_b200 import abi as _abi
+        d.precision = _abi.PRECISION_MIXED
     cfl = WORKLOADS[args.workload][1]
     ncell, V = d.ncell, d.nvar
     state_bytes = ncell * V * 8
@@ -247,6 +252,7 @@ def run_ours(args):
     evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     s.profile(True)
+    k0 = native.lib().dimgpu_kernel_launches()
     with ClockSampler(local) as clk, torch.cuda.stream(stream):
         for k in range(args.steps):
             if flush is not None:
@@ -256,6 +262,7 @@ def run_ours(args):
             evs[k][1].record(stream)
         stream.synchronize()
     barrier()
+    kernels_timed = native.lib().dimgpu_kernel_launches() - k0
     step_ms = [a.elapsed_time(b) for a, b in evs]
     prof = s.profile_read()
     s.profile(False)
@@ -275,6 +282,7 @@ def run_ours(args):
             s.enqueue_steps(1, cfl, 1e300)
             s.collect()
             s.download(pin_out.numpy().reshape(V, ncell))
+            pin_in, pin_out = pin_out, pin_in
         barrier()
         for k in range(args.steps):
             if flush is not None:
@@ -296,6 +304,22 @@ def run_ours(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         total_ms, e2e_ms = float(t[0]), float(t[1])
 
+    error_vs_fp64 = None
+    if args.precision == "mixed":
+        # the FP64 path is bit-identical to the oracle: compare the mixed
+        # state after the same warm-up + timed + e2e steps with it
+        mixed_out = s.download()
+        nsteps = args.warmup + args.steps + max(1, args.warmup) + args.steps
+        d64 = d.copy()
+        d64.precision = 0
+        with Session(d64, U) as s64:
+            s64.steps(nsteps, cfl, 1e300)
+            ref = s64.download()
+        den = np.abs(ref).sum(axis=1)
+        l1 = np.abs(mixed_out - ref).sum(axis=1) / np.where(den > 0, den, 1.0)
+        linf = np.abs(mixed_out - ref).max(axis=1) / np.maximum(np.abs(ref).max(axis=1), 1e-300)
+        error_vs_fp64 = {"steps": nsteps, "rel_l1_per_variable": [float(x) for x in l1],
+                         "rel_linf_per_variable": [float(x) for x in linf], "max_rel_l1": float(l1.max())}
     s.close()
     if rank != 0:
         if world > 1:
@@ -309,8 +333,9 @@ def run_ours(args):
     alg_bytes = 2 * V * 8 * ncell  # read + write of the state, per sweep launch
     achieved = alg_bytes / avg_sweep_s / 1e9
     peak, peak_src = measured_peaks()
-    traffic, traffic_src = ncu_traffic(args.workload)
-    launches = sum(v["launches"] for v in prof.values())
+    traffic, traffic_src = ncu_traffic(args.workload + ("-mixed" if args.precision == "mixed" else ""))
+    sched = "mixed staged sweep (staged_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
+        "staged sweep (staged_a..staged_e)"
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -324,7 +349,7 @@ def run_ours(args):
         },
         "roofline": {
             "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": "sweep_kernel",
+            "traffic": traffic, "kernel": sched,
             "note": f"algorithmic {alg_bytes} B per sweep launch (2*V*8*cells); avg sweep "
                     f"{avg_sweep_s * 1e3:.4f} ms over {sweep['launches']} launches; peak {peak_src}"
                     + (f"; traffic from {traffic_src}" if traffic_src else ""),
@@ -332,9 +357,13 @@ def run_ours(args):
         "phase_ms": {k: v["ms"] for k, v in prof.items()},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * ncell * 8,
                 "d2h_bytes_per_step": V * ncell * 8 + 8},
-        "gpu_launches": launches,
+        "gpu_launches": kernels_timed,
         "clocks": clocks,
     }
+    if error_vs_fp64 is not None:
+        line["dtype"] = "f64 state / f32 flux"
+        line["precision"] = "mixed"
+        line["error_vs_fp64_oracle"] = error_vs_fp64
     if world == 1 and not args.no_cpu:
         cb = cpu_reference_rate(args.workload, steps=2 if args.workload != "c0" else 20, warmup=0)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -481,6 +510,7 @@ def main():
     ap.add_argument("--workload", default="c1", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--scale", type=int, default=1, help="divide the grid sides (profiling runs)")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--c3-steps", type=int, default=500)
     ap.add_argument("--c3-instances", type=int, default=256)
     ap.add_argument("--c3-sequential", type=int, default=16, help="instances in the sequential sample")

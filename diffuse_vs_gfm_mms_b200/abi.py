@@ -54,6 +54,9 @@ SCHEDULE_STAGED = 1
 TIME_SPLIT = 0
 TIME_UNSPLIT = 1
 
+MODEL_DIM = 0     # the five-equation diffuse-interface step
+MODEL_EULER = 1   # the single-material Euler step (one material, no level set)
+
 
 class Material(C.Structure):
     _fields_ = [("kind", C.c_int), ("gamma", C.c_double), ("p_inf", C.c_double)]
@@ -72,6 +75,7 @@ class Desc(C.Structure):
         ("alpha_source_floor", C.c_double),
         ("precision", C.c_int),
         ("time_update", C.c_int),
+        ("model", C.c_int),
     ]
 
     @property
@@ -112,7 +116,7 @@ def bc_code(name) -> int:
 def make_desc(dim: int, N: Sequence[int], dx: Sequence[float],
               materials: Sequence[tuple], bc_lo=None, bc_hi=None,
               lambda_model="kapila", alpha_source_floor: float = 0.0,
-              precision: int = PRECISION_FP64, time_update="split") -> Desc:
+              precision: int = PRECISION_FP64, time_update="split", model: int = MODEL_DIM) -> Desc:
     """Build a descriptor.  materials: (kind, gamma, p_inf) with kind a name or code."""
     if dim not in (1, 2, 3):
         raise ValueError("dim must be 1, 2 or 3")
@@ -141,6 +145,7 @@ def make_desc(dim: int, N: Sequence[int], dx: Sequence[float],
     if isinstance(time_update, str):
         time_update = TIME_UNSPLIT if time_update.lower() == "unsplit" else TIME_SPLIT
     d.time_update = int(time_update)
+    d.model = int(model)
     return d
 
 

@@ -24,9 +24,10 @@ NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
          "-ccbin", "g++", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
-SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "dimgpu_api.cu", "dimgpu_noalloc.cu",
-           "dimgpu_batch.cu"]
-HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h", "dim_batch.cuh"]
+SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "inst_euler.cu", "dimgpu_api.cu",
+           "dimgpu_noalloc.cu", "dimgpu_batch.cu"]
+HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h", "dim_batch.cuh", "dim_mixed.h",
+           "euler_physics.h", "euler_kernels.cuh"]
 
 
 def _mtime(p):

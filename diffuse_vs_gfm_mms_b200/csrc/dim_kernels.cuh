@@ -10,6 +10,7 @@
 
 #include "dim_launch.h"
 #include "dim_line.h"
+#include "dim_mixed.h"
 #include "dimgpu.h"
 
 namespace dimgpu {
@@ -404,21 +405,52 @@ struct StagedItem {
     }
 };
 
+// Optional CFL reduction fused into stage A of the first sweep of a step:
+// stage A recovers every cell's primitive from the very state the CFL
+// minimum is taken over, so the candidate costs one sound speed, not a
+// second recovery.  Block minima go to one slot by atomicMin on the bit
+// pattern (every candidate is a non-negative double or +inf, which order
+// like their bits).
+struct FusedCfl {
+    int on;
+    int unsplit;
+    double cfl;
+    unsigned long long* slot;
+};
+
+__device__ __forceinline__ void fused_cfl_reduce(double best, const FusedCfl& c)
+{
+    __shared__ double red[8];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) best = dmin(best, __shfl_xor_sync(0xffffffffu, best, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = best;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double m = red[0];
+        for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = dmin(m, red[w]);
+        atomicMin(c.slot, (unsigned long long)__double_as_longlong(m));
+    }
+}
+
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) staged_a(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
-                                                StagedBufs<NM, D> b)
+                                                StagedBufs<NM, D> b, FusedCfl fc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)ls.nl * ls.n) return;
-    const StagedItem<DIR> it(g, ls, t);
-    State<NM, D> U;
-    load_cell<NM, D>(in, g.ncell, it.cell, U);
-    CellA<NM, D> A;
-    stage_a<NM, D>(M, U, A);
-    g_put<NM, D>(b.P, b.cap, t, A.P);
-    g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
+    double best = HUGE_VAL;
+    if (t < (long long)ls.nl * ls.n) {
+        const StagedItem<DIR> it(g, ls, t);
+        State<NM, D> U;
+        load_cell<NM, D>(in, g.ncell, it.cell, U);
+        CellA<NM, D> A;
+        stage_a<NM, D>(M, U, A);
+        g_put<NM, D>(b.P, b.cap, t, A.P);
+        g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
-    for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
+        for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
+        if (fc.on) best = cfl_candidate<NM, D>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+    }
+    if (fc.on) fused_cfl_reduce(best, fc);
 }
 
 template<int NM, int D, int DIR>
@@ -523,6 +555,95 @@ __global__ void __launch_bounds__(256) staged_e(const double* __restrict__ in, d
     State<NM, D> Un;
     stage_e<NM, D>(M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, *dtp, g.dx[DIR], Un);
     store_cell<NM, D>(out, g.ncell, it.cell, Un);
+}
+
+// ---- the mixed-precision staged sweep (precision MIXED) ---------------------------
+//
+// Stage A and stage E are staged_a / staged_e (FP64 cell recovery, FP64 cell
+// update).  mixed_b is stage B with FP32-limited slopes and no face-state
+// round trip; mixed_cd builds the two face states of face i|i+1 from the
+// half-step primitives of cells i-1..i+2 and runs the FP32-increment HLLC,
+// so the face states never reach HBM.  Scratch: P, ck, Pe, Ph and the face
+// records, at the staged positions.
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) mixed_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                               StagedBufs<NM, D> b, const double* __restrict__ dtp)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
+    CellA<NM, D> A;
+    g_get<NM, D>(b.Pe, b.cap, t, A.Pe);
+    Prim<NM, D> Ph;
+    if (end) {
+        Ph = A.Pe;
+    }
+    else {
+        State<NM, D> U;
+        load_cell<NM, D>(in, g.ncell, it.cell, U);
+#pragma unroll
+        for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
+        Prim<NM, D> lo, hi;
+        g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
+        g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+        stage_b_mixed<NM, D>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
+    }
+    g_put<NM, D>(b.Ph, b.cap, t, Ph);
+}
+
+// Face state of cell item t on the given side (end cells: U and P).
+template<int NM, int D, int DIR>
+__device__ __forceinline__ void mixed_face(const double* __restrict__ in, const Grid& g, const Mats& M,
+                                           const StagedBufs<NM, D>& b, const StagedItem<DIR>& it, long long t, int n,
+                                           bool right, State<NM, D>& Uf, Prim<NM, D>& Pf)
+{
+    const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
+    if (end) {
+        load_cell<NM, D>(in, g.ncell, it.cell, Uf);
+        g_get<NM, D>(b.P, b.cap, t, Pf);
+        return;
+    }
+    Prim<NM, D> lo, c, hi;
+    g_get<NM, D>(b.Ph, b.cap, t - it.s, lo);
+    g_get<NM, D>(b.Ph, b.cap, t, c);
+    g_get<NM, D>(b.Ph, b.cap, t + it.s, hi);
+    face_mixed<NM, D>(M, lo, c, hi, right, Uf, Pf);
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) mixed_cd(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                                StagedBufs<NM, D> b, int* __restrict__ err)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    if (it.gi >= n - 1) return;  // face i|i+1 exists for i <= n-2
+    State<NM, D> UL, UR;
+    Prim<NM, D> PL, PR;
+    mixed_face<NM, D, DIR>(in, g, M, b, it, t, n, true, UL, PL);
+    StagedItem<DIR> nx = it;
+    nx.gi += 1;
+    nx.cell += g.stride[DIR];
+    mixed_face<NM, D, DIR>(in, g, M, b, nx, t + it.s, n, false, UR, PR);
+    FaceD<NM, D> f;
+    if (!stage_d_mixed<NM, D>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    g_put<NM, D>(b.F, b.cap, t, f);
+}
+
+// dt = min(dt_max, slot) after a fused stage A; re-arms the slot to +inf.
+static __global__ void fused_cfl_finalize(unsigned long long* __restrict__ slot, double dt_max, double* __restrict__ dt,
+                                   double* __restrict__ hist, int* __restrict__ err)
+{
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const double m = __longlong_as_double((long long)*slot);
+    const double d = dmin(dt_max, m);
+    dt[0] = d;
+    if (hist) hist[0] = d;
+    if (!(d > 0.0) || !fin(d)) atomicOr(err, kErrDt);
+    *slot = (unsigned long long)__double_as_longlong(HUGE_VAL);
 }
 
 // ---- CFL ------------------------------------------------------------------------
@@ -804,6 +925,7 @@ cudaError_t launch_sweep_dir(const Grid& g, const Mats& M, Tile tile, const doub
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -826,7 +948,7 @@ cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const
 // holds kStagedVars(NM, D) * cap doubles.
 template<int NM, int D, int DIR>
 cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, double* out, const double* dt, int* err,
-                              double* scratch, long long cap, cudaStream_t s)
+                              double* scratch, long long cap, const FusedStep& fs, cudaStream_t s)
 {
     const int n = g.N[DIR];
     const long long nlines = g.ncell / n;
@@ -851,11 +973,19 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         ls.n = n;
         const long long items = (long long)ls.nl * n;
         const unsigned blocks = (unsigned)((items + 255) / 256);
-        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b);
+        FusedCfl fc{0, 0, 0.0, nullptr};
+        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
+        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
+        count_launches(1);
+        if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
         staged_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        count_launches(1);
         staged_c<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b);
+        count_launches(1);
         staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
+        count_launches(1);
         staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
+        count_launches(1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
     }
@@ -864,14 +994,74 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
 
 template<int NM, int D>
 cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const double* in, double* out,
-                                const double* dt, int* err, double* scratch, long long cap, cudaStream_t s)
+                                const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
+                                cudaStream_t s)
 {
-    if (dir == 0) return launch_staged_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, s);
+    if (fs.on && (long long)g.ncell > cap) return cudaErrorInvalidValue;  // fusion needs a single chunk
+    if (dir == 0) return launch_staged_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, fs, s);
     if constexpr (D >= 2) {
-        if (dir == 1) return launch_staged_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, s);
+        if (dir == 1) return launch_staged_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, fs, s);
     }
     if constexpr (D >= 3) {
-        if (dir == 2) return launch_staged_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, s);
+        if (dir == 2) return launch_staged_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, fs, s);
+    }
+    return cudaErrorInvalidValue;
+}
+
+template<int NM, int D, int DIR>
+cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, double* out, const double* dt, int* err,
+                             double* scratch, long long cap, const FusedStep& fs, cudaStream_t s)
+{
+    const int n = g.N[DIR];
+    const long long nlines = g.ncell / n;
+    const long long per = cap / n;
+    if (per < 1) return cudaErrorInvalidValue;
+    StagedBufs<NM, D> b;
+    b.cap = cap;
+    double* p = scratch;
+    b.P = p; p += kPrimVars(NM, D) * cap;
+    b.ck = p; p += NM * cap;
+    b.Pe = p; p += kPrimVars(NM, D) * cap;
+    b.Ph = p; p += kPrimVars(NM, D) * cap;
+    b.F = p;
+    b.LS = b.RS = nullptr;
+    b.PLS = b.PRS = nullptr;
+    for (long long L0 = 0; L0 < nlines; L0 += per) {
+        LineSet ls;
+        ls.L0 = L0;
+        ls.nl = (int)((nlines - L0 < per) ? (nlines - L0) : per);
+        ls.n = n;
+        const long long items = (long long)ls.nl * n;
+        const unsigned blocks = (unsigned)((items + 255) / 256);
+        FusedCfl fc{0, 0, 0.0, nullptr};
+        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
+        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
+        count_launches(1);
+        if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
+        mixed_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        count_launches(1);
+        mixed_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+        count_launches(1);
+        staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
+        count_launches(1);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+template<int NM, int D>
+cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const double* in, double* out,
+                               const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
+                               cudaStream_t s)
+{
+    if (fs.on && (long long)g.ncell > cap) return cudaErrorInvalidValue;
+    if (dir == 0) return launch_mixed_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, fs, s);
+    if constexpr (D >= 2) {
+        if (dir == 1) return launch_mixed_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, fs, s);
+    }
+    if constexpr (D >= 3) {
+        if (dir == 2) return launch_mixed_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, fs, s);
     }
     return cudaErrorInvalidValue;
 }
@@ -885,6 +1075,7 @@ cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double
     if (nb < 1) nb = 1;
     *nblocks = (int)nb;
     cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, blockmin);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -902,6 +1093,7 @@ cudaError_t launch_bc(const Grid& g, const Mats& M, double* state, cudaStream_t 
     if (nonreflective && three) serial = true;
     if (serial) {
         bc_serial_kernel<NM, D><<<1, 1, 0, s>>>(state, g, M);
+        count_launches(1);
         return cudaGetLastError();
     }
     long long plane[3] = {0, 0, 0};
@@ -918,6 +1110,7 @@ cudaError_t launch_bc(const Grid& g, const Mats& M, double* state, cudaStream_t 
     }
     if (total == 0) return cudaSuccess;
     bc_kernel<NM, D><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(state, g, M, plane[0], plane[1], plane[2]);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -926,6 +1119,7 @@ cudaError_t launch_accumulate(const Grid& g, const Mats& M, double* accum, const
                               const double* base, cudaStream_t s)
 {
     accumulate_kernel<NM, D><<<(unsigned)((g.ncell + 255) / 256), 256, 0, s>>>(accum, dir_state, base, g, M);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -938,6 +1132,7 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
     if (nb < 1) nb = 1;
     *nblocks = (int)nb;
     totals_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, volume, partial);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -945,7 +1140,11 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
     template cudaError_t launch_sweep<NM, D>(const Grid&, const Mats&, int, Tile, const double*, double*,    \
                                              const double*, int*, cudaStream_t);                             \
     template cudaError_t launch_sweep_staged<NM, D>(const Grid&, const Mats&, int, const double*, double*,   \
-                                                    const double*, int*, double*, long long, cudaStream_t);  \
+                                                    const double*, int*, double*, long long, const FusedStep&, \
+                                                    cudaStream_t);                                           \
+    template cudaError_t launch_sweep_mixed<NM, D>(const Grid&, const Mats&, int, const double*, double*,    \
+                                                   const double*, int*, double*, long long, const FusedStep&, \
+                                                   cudaStream_t);                                            \
     template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
                                            int, int*, cudaStream_t);                                         \
     template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \

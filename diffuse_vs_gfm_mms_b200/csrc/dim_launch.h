@@ -17,6 +17,12 @@ enum : int {
     kErrDt = 2,         // CFL step is not positive and finite
 };
 
+// Kernels launched by this library so far, process-wide (read with
+// dimgpu_kernel_launches).  Every launch site adds its count; a batch adds,
+// per step, the kernels one step holds, whether launched directly or
+// replayed from a captured graph.
+void count_launches(long long n);
+
 struct Grid {
     int N[3];
     long long ncell;
@@ -36,14 +42,36 @@ template<int NM, int D>
 cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const double* in, double* out,
                          const double* dt, int* err, cudaStream_t s);
 
+// CFL reduction fused into stage A of a staged / mixed sweep: when `on`, the
+// launcher reduces the CFL minimum into `slot` during stage A and writes
+// dt = min(dt_max, minimum) to dt[0] (and hist[0]) before stage B.  Needs
+// the grid to fit one scratch chunk.
+struct FusedStep {
+    int on;
+    int unsplit;
+    double cfl;
+    double dt_max;
+    unsigned long long* slot;
+    double* dt;
+    double* hist;
+    int* err;
+};
+
 // The staged schedule of the same sweep: stages A..E as separate kernels
 // over chunks of whole lines of at most `cap` cells, intermediates in
 // `scratch` (staged_scratch_doubles(nmat, dim) * cap doubles).
 template<int NM, int D>
 cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const double* in, double* out,
-                                const double* dt, int* err, double* scratch, long long cap, cudaStream_t s);
+                                const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
+                                cudaStream_t s);
 
 int staged_scratch_doubles(int nmat, int dim);
+
+// Mixed-precision staged sweep (dim_mixed.h): same scratch as the staged one.
+template<int NM, int D>
+cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const double* in, double* out,
+                               const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
+                               cudaStream_t s);
 
 // Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
 template<int NM, int D>
@@ -102,6 +130,26 @@ template<int NM, int D>
 cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s);
 
 int sweep_smem_doubles(int nmat, int dim);
+
+// ---- the single-material Euler step (euler_kernels.cuh) ----
+// One split sweep (fused tile kernel); end cells of each line get zeros
+// (ends_copy 0, the split update) or their input state (1, unsplit).
+template<int D>
+cudaError_t launch_euler_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const double* in, double* out,
+                               const double* dt, int* err, int ends_copy, cudaStream_t s);
+
+// Per-block CFL minima (finished by launch_cfl_finalize).
+template<int D>
+cudaError_t launch_euler_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
+                             double* blockmin, int max_blocks, int* nblocks, int* err, cudaStream_t s);
+
+template<int D>
+cudaError_t launch_euler_bc(const Grid& g, const Mats& M, double* state, cudaStream_t s);
+
+// acc = acc + (dir - base); with `enforce`, then enforce_positive_conserved.
+template<int D>
+cudaError_t launch_euler_accumulate(const Grid& g, const Mats& M, double* acc, const double* dir_state,
+                                    const double* base, bool enforce, cudaStream_t s);
 
 // Message returned by dimgpu_last_error(NULL) on the calling thread.
 void set_sessionless_error(const std::string& msg);

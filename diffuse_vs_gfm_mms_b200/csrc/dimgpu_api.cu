@@ -1,6 +1,7 @@
 // dimgpu_api.cu — the C-ABI (include/dimgpu.h): sessions owning the
 // device-resident SoA state, the step orchestration of dim::advance_one_step
 // (src/dim/solver/advance_step.hpp:150-270) and the stateless drop-in call.
+#include <atomic>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -46,6 +47,16 @@ int fail(std::string* where, int code, const std::string& msg)
         default: e = cudaErrorInvalidValue; break;                                  \
     }
 
+#define DISPATCH_D(dim, ...)                                                        \
+    switch (dim) {                                                                  \
+        case 1: { constexpr int D = 1; __VA_ARGS__; } break;                        \
+        case 2: { constexpr int D = 2; __VA_ARGS__; } break;                        \
+        case 3: { constexpr int D = 3; __VA_ARGS__; } break;                        \
+        default: e = cudaErrorInvalidValue; break;                                  \
+    }
+
+bool is_euler(const dimgpu_desc& d) { return d.model == DIMGPU_MODEL_EULER; }
+
 __device__ __forceinline__ double warp_min_f(double v)
 {
 #pragma unroll
@@ -78,10 +89,15 @@ __global__ void cfl_finalize_kernel(const double* __restrict__ blockmin, int nb,
 
 namespace dimgpu {
 
+std::atomic<long long> g_launches{0};
+
+void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
 cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_max, double* dt, double* hist,
                                 int* err, cudaStream_t s)
 {
     cfl_finalize_kernel<<<1, 256, 0, s>>>(blockmin, nblocks, dt_max, dt, hist, err);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -115,6 +131,7 @@ struct dimgpu_session {
     Tile tile[3] = {{128, 1}, {64, 4}, {64, 4}};
     int schedule[3] = {DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED};
     double* staged = nullptr;  // scratch of the staged schedule (allocated on first use)
+    unsigned long long* cfl_slot = nullptr;  // fused CFL minimum (bit pattern of a double)
     long long staged_cap = 0;
     std::string msg;
     // profiling
@@ -205,10 +222,21 @@ int validate_desc(const dimgpu_desc* d, std::string* where)
     }
     if (d->lambda_model < 0 || d->lambda_model > 2)
         return fail(where, DIMGPU_E_INVALID_ARG, "dim::alpha_rhs_coefficients: unknown lambda model");
-    if (d->precision != DIMGPU_PRECISION_FP64)
-        return fail(where, DIMGPU_E_UNSUPPORTED, "this build runs precision FP64 only");
+    if (d->precision != DIMGPU_PRECISION_FP64 && d->precision != DIMGPU_PRECISION_MIXED)
+        return fail(where, DIMGPU_E_INVALID_ARG, "precision must be DIMGPU_PRECISION_FP64 or _MIXED");
     if (d->time_update != DIMGPU_TIME_SPLIT && d->time_update != DIMGPU_TIME_UNSPLIT)
         return fail(where, DIMGPU_E_INVALID_ARG, "time_update must be split or unsplit");
+    if (d->model != DIMGPU_MODEL_DIM && d->model != DIMGPU_MODEL_EULER)
+        return fail(where, DIMGPU_E_INVALID_ARG, "model must be DIMGPU_MODEL_DIM or DIMGPU_MODEL_EULER");
+    if (d->model == DIMGPU_MODEL_EULER) {
+        if (d->nmat != 1)
+            return fail(where, DIMGPU_E_INVALID_ARG, "the Euler step runs exactly one material (nmat = 1)");
+        if (d->precision != DIMGPU_PRECISION_FP64)
+            return fail(where, DIMGPU_E_UNSUPPORTED, "the Euler step runs in FP64 only");
+        for (int a = 0; a < d->dim; ++a)
+            if (d->N[a] < 3)
+                return fail(where, DIMGPU_E_INVALID_ARG, "reconstruct_line_interfaces: need at least 3 cells");
+    }
     return DIMGPU_OK;
 }
 
@@ -220,6 +248,9 @@ int check_err(dimgpu_session* s)
     if (e != cudaSuccess) return cuda_fail(s, e, "step");
     if (h) {
         cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+        if ((h & kErrNonFinite) && is_euler(s->desc))
+            return fail(&s->msg, DIMGPU_E_NONFINITE,
+                        "hllc_flux_normal: invalid star state, or non-finite density (require_positive)");
         if (h & kErrNonFinite)
             return fail(&s->msg, DIMGPU_E_NONFINITE, "dim::hllc_flux_normal: invalid density or pressure (non-finite)");
         if (h & kErrDt) return fail(&s->msg, DIMGPU_E_NONFINITE, "run_dim_case: non-positive timestep");
@@ -235,9 +266,15 @@ cudaError_t run_cfl(dimgpu_session* s, double cfl, double dt_max, double* hist)
     {
         ProfScope p(s, kCfl);
         const bool unsplit = s->desc.time_update == DIMGPU_TIME_UNSPLIT;
-        DISPATCH_ND(s->desc.nmat, s->desc.dim,
-                    e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks,
-                                          &nb, s->stream));
+        if (is_euler(s->desc)) {
+            DISPATCH_D(s->desc.dim, e = launch_euler_cfl<D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin,
+                                                            kMaxCflBlocks, &nb, s->err, s->stream));
+        }
+        else {
+            DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                        e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks,
+                                              &nb, s->stream));
+        }
     }
     if (e != cudaSuccess) return e;
     ProfScope p(s, kOther);
@@ -258,9 +295,27 @@ cudaError_t ensure_staged_scratch(dimgpu_session* s)
     return e;
 }
 
-cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out)
+cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out, const FusedStep* fused = nullptr,
+                      int ends_copy = 0)
 {
     cudaError_t e = cudaSuccess;
+    const FusedStep off{0, 0, 0.0, 0.0, nullptr, nullptr, nullptr, nullptr};
+    const FusedStep& fs = fused ? *fused : off;
+    if (is_euler(s->desc)) {
+        ProfScope p(s, kSweep);
+        DISPATCH_D(s->desc.dim, e = launch_euler_sweep<D>(s->g, s->M, dir, s->tile[dir], in, out, s->dt, s->err,
+                                                          ends_copy, s->stream));
+        return e;
+    }
+    if (s->desc.precision == DIMGPU_PRECISION_MIXED) {
+        e = ensure_staged_scratch(s);
+        if (e != cudaSuccess) return e;
+        ProfScope p(s, kSweep);
+        DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                    e = launch_sweep_mixed<NM, D>(s->g, s->M, dir, in, out, s->dt, s->err, s->staged,
+                                                  s->staged_cap, fs, s->stream));
+        return e;
+    }
     if (s->schedule[dir] == DIMGPU_SCHEDULE_STAGED) {
         e = ensure_staged_scratch(s);
         if (e != cudaSuccess) return e;
@@ -269,7 +324,7 @@ cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out)
     if (s->schedule[dir] == DIMGPU_SCHEDULE_STAGED) {
         DISPATCH_ND(s->desc.nmat, s->desc.dim,
                     e = launch_sweep_staged<NM, D>(s->g, s->M, dir, in, out, s->dt, s->err, s->staged,
-                                                   s->staged_cap, s->stream));
+                                                   s->staged_cap, fs, s->stream));
         return e;
     }
     DISPATCH_ND(s->desc.nmat, s->desc.dim,
@@ -281,6 +336,10 @@ cudaError_t run_bc(dimgpu_session* s, double* st)
 {
     cudaError_t e = cudaSuccess;
     ProfScope p(s, kBoundary);
+    if (is_euler(s->desc)) {
+        DISPATCH_D(s->desc.dim, e = launch_euler_bc<D>(s->g, s->M, st, s->stream));
+        return e;
+    }
     DISPATCH_ND(s->desc.nmat, s->desc.dim, e = launch_bc<NM, D>(s->g, s->M, st, s->stream));
     return e;
 }
@@ -309,16 +368,60 @@ cudaError_t run_directions(dimgpu_session* s)
     for (int dir = 0; dir < D && e == cudaSuccess; ++dir) {
         const double* dstate = s->buf[base];
         if (s->g.N[dir] > 1) {
-            e = run_sweep(s, dir, s->buf[base], s->buf[2]);
+            e = run_sweep(s, dir, s->buf[base], s->buf[2], nullptr, 1);
             dstate = s->buf[2];
         }
         if (e != cudaSuccess) break;
         ProfScope p(s, kOther);
-        DISPATCH_ND(s->desc.nmat, s->desc.dim,
-                    e = launch_accumulate<NM, D>(s->g, s->M, s->buf[acc], dstate, s->buf[base], s->stream));
+        if (is_euler(s->desc)) {
+            // advance_step.hpp:617-641: accumulate every axis, enforce once after the last
+            DISPATCH_D(s->desc.dim, e = launch_euler_accumulate<D>(s->g, s->M, s->buf[acc], dstate, s->buf[base],
+                                                                   dir == D - 1, s->stream));
+        }
+        else {
+            DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                        e = launch_accumulate<NM, D>(s->g, s->M, s->buf[acc], dstate, s->buf[base], s->stream));
+        }
     }
     if (e == cudaSuccess) e = run_bc(s, s->buf[acc]);
     s->cur = acc;
+    return e;
+}
+
+// One time step: the CFL dt, then the directions.  When the first sweep is
+// staged (or mixed), split and the grid fits one scratch chunk, the CFL
+// minimum is reduced inside that sweep's stage A instead of by a separate
+// recovery pass over the state.
+cudaError_t run_step(dimgpu_session* s, double cfl, double dt_max, double* hist)
+{
+    const bool fusable = !is_euler(s->desc) && s->desc.time_update == DIMGPU_TIME_SPLIT && s->g.N[0] > 1 &&
+                         s->cfl_slot &&
+                         (s->desc.precision == DIMGPU_PRECISION_MIXED ||
+                          s->schedule[0] == DIMGPU_SCHEDULE_STAGED) &&
+                         s->ncell <= kStagedChunkCells;
+    if (!fusable) {
+        cudaError_t e = run_cfl(s, cfl, dt_max, hist);
+        if (e == cudaSuccess) e = run_directions(s);
+        return e;
+    }
+    cudaError_t e = ensure_staged_scratch(s);
+    if (e != cudaSuccess) return e;
+    if (s->ncell > s->staged_cap) {
+        e = run_cfl(s, cfl, dt_max, hist);
+        if (e == cudaSuccess) e = run_directions(s);
+        return e;
+    }
+    const FusedStep fs{1, 0, cfl, dt_max, s->cfl_slot, s->dt, hist, s->err};
+    e = run_sweep(s, 0, s->buf[s->cur], s->buf[1 - s->cur], &fs);
+    s->cur = 1 - s->cur;
+    if (e == cudaSuccess) e = run_bc(s, s->buf[s->cur]);
+    for (int dir = 1; dir < s->desc.dim && e == cudaSuccess; ++dir) {
+        if (s->g.N[dir] > 1) {
+            e = run_sweep(s, dir, s->buf[s->cur], s->buf[1 - s->cur]);
+            s->cur = 1 - s->cur;
+        }
+        if (e == cudaSuccess) e = run_bc(s, s->buf[s->cur]);
+    }
     return e;
 }
 
@@ -377,6 +480,11 @@ int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
     if (e == cudaSuccess) e = cudaMalloc(&s->hist, sizeof(double) * kHistCap);
     if (e == cudaSuccess) e = cudaMalloc(&s->partial, sizeof(double) * kTotalsBlocks * (DIMGPU_MAX_MATERIALS + 5));
     if (e == cudaSuccess) e = cudaMalloc(&s->err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&s->cfl_slot, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        const double inf = HUGE_VAL;
+        e = cudaMemcpyAsync(s->cfl_slot, &inf, sizeof inf, cudaMemcpyHostToDevice, s->stream);
+    }
     if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
@@ -404,6 +512,7 @@ int dimgpu_destroy(dimgpu_session* s)
     cudaFree(s->partial);
     cudaFree(s->err);
     cudaFree(s->staged);
+    cudaFree(s->cfl_slot);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     delete s;
     return DIMGPU_OK;
@@ -477,8 +586,7 @@ int dimgpu_step(dimgpu_session* s, double cfl, double dt_max, double* dt_out, di
         std::memcpy(before, s->prof, sizeof before);
         s->profiling = true;
     }
-    cudaError_t e = run_cfl(s, cfl, dt_max, nullptr);
-    if (e == cudaSuccess) e = run_directions(s);
+    cudaError_t e = run_step(s, cfl, dt_max, nullptr);
     double h = 0.0;
     if (e == cudaSuccess) e = cudaMemcpyAsync(&h, s->dt, sizeof(double), cudaMemcpyDeviceToHost, s->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
@@ -511,8 +619,7 @@ int dimgpu_enqueue_steps(dimgpu_session* s, int n, double cfl, double dt_max)
         return fail(&s->msg, DIMGPU_E_INVALID_ARG, "more than 4096 steps enqueued: call dimgpu_collect first");
     cudaError_t e = cudaSuccess;
     for (int k = 0; k < n && e == cudaSuccess; ++k) {
-        e = run_cfl(s, cfl, dt_max, s->hist + s->pending);
-        if (e == cudaSuccess) e = run_directions(s);
+        e = run_step(s, cfl, dt_max, s->hist + s->pending);
         if (e == cudaSuccess) ++s->pending;
     }
     return e == cudaSuccess ? DIMGPU_OK : cuda_fail(s, e, "dimgpu_enqueue_steps");
@@ -607,6 +714,8 @@ int dimgpu_profile(dimgpu_session* s, int enable)
     s->profiling = enable != 0;
     return DIMGPU_OK;
 }
+
+long long dimgpu_kernel_launches(void) { return g_launches.load(std::memory_order_relaxed); }
 
 int dimgpu_profile_read(dimgpu_session* s, double* out8)
 {

@@ -279,6 +279,7 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
         return bfail(b, DIMGPU_E_INVALID_ARG, "instance nmat / dim differ from the batch's");
     if (d->time_update != DIMGPU_TIME_SPLIT) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs split steps only");
     if (d->precision != DIMGPU_PRECISION_FP64) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs FP64 only");
+    if (d->model != DIMGPU_MODEL_DIM) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs the DIM step only");
     if (steps < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative step count");
     if (!(cfl > 0.0) || !(dt_max > 0.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "cfl and dt_max must be positive");
     long long ncell = 1;
@@ -400,10 +401,12 @@ int dimgpu_batch_run(dimgpu_batch* b, int n)
                 if (e != cudaSuccess) break;
             }
             e = cudaGraphLaunch(g, b->stream);
+            count_launches((long long)kGraphSteps * (2 + 6 * b->dim));  // batch_step: cfl, finalize, 6 per axis
             done += kGraphSteps;  // kGraphSteps is even: the parity is unchanged
         }
         else {
             e = one_step(b, L, b->parity);
+            count_launches(2 + 6 * b->dim);
             if (odd) b->parity = 1 - b->parity;
             done += 1;
         }

@@ -97,6 +97,10 @@ extern "C" int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const doub
     }
     if (desc->lambda_model < 0 || desc->lambda_model > 2)
         return noalloc_fail(DIMGPU_E_INVALID_ARG, "unknown lambda model");
+    if (desc->model != DIMGPU_MODEL_DIM && desc->model != DIMGPU_MODEL_EULER)
+        return noalloc_fail(DIMGPU_E_INVALID_ARG, "unknown model");
+    if (desc->model == DIMGPU_MODEL_EULER && desc->nmat != 1)
+        return noalloc_fail(DIMGPU_E_INVALID_ARG, "the Euler step runs exactly one material");
     if (!(cfl > 0.0)) return noalloc_fail(DIMGPU_E_INVALID_ARG, "cfl must be positive");
     if (!(dt_max > 0.0)) return noalloc_fail(DIMGPU_E_INVALID_ARG, "dt_max must be positive");
 
@@ -133,7 +137,15 @@ extern "C" int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const doub
     cudaError_t e = cudaMemsetAsync(err, 0, sizeof(int), s);
     int nb = 1;
     const bool unsplit = desc->time_update == DIMGPU_TIME_UNSPLIT;
-    if (e == cudaSuccess) {
+    if (e == cudaSuccess && desc->model == DIMGPU_MODEL_EULER) {
+        switch (desc->dim) {
+            case 1: e = launch_euler_cfl<1>(g, M, d_state, cfl, unsplit, blockmin, kScratchSlots, &nb, err, s); break;
+            case 2: e = launch_euler_cfl<2>(g, M, d_state, cfl, unsplit, blockmin, kScratchSlots, &nb, err, s); break;
+            case 3: e = launch_euler_cfl<3>(g, M, d_state, cfl, unsplit, blockmin, kScratchSlots, &nb, err, s); break;
+            default: e = cudaErrorInvalidValue; break;
+        }
+    }
+    else if (e == cudaSuccess) {
         switch (desc->nmat * 10 + desc->dim) {
 #define NOALLOC_CASE(NM, D) \
             case NM * 10 + D: e = launch_cfl<NM, D>(g, M, d_state, cfl, unsplit, blockmin, kScratchSlots, &nb, s); break;
@@ -146,11 +158,15 @@ extern "C" int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const doub
         }
     }
     if (e == cudaSuccess) e = launch_cfl_finalize(blockmin, nb, dt_max, dt_dev, nullptr, err, s);
-    double dt = 0.0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&dt, dt_dev, sizeof(double), cudaMemcpyDeviceToHost, s);
+    double dt_and_flag[2] = {0.0, 0.0};  // dt, then the error-flag slot
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dt_and_flag, dt_dev, 2 * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return noalloc_fail(DIMGPU_E_CUDA, std::string("dimgpu_compute_dt_cfl_noalloc: ") +
                                                                  cudaGetErrorString(e));
-    *dt_out = dt;
+    int flag = 0;
+    std::memcpy(&flag, &dt_and_flag[1], sizeof flag);
+    if (desc->model == DIMGPU_MODEL_EULER && (flag & kErrNonFinite))
+        return noalloc_fail(DIMGPU_E_NONFINITE, "thermo: invalid density (non-finite)");
+    *dt_out = dt_and_flag[0];
     return DIMGPU_OK;
 }

@@ -36,6 +36,7 @@ SIGNATURES = {
     "dimgpu_set_schedule": ([_S, C.c_int, C.c_int], C.c_int),
     "dimgpu_profile": ([_S, C.c_int], C.c_int),
     "dimgpu_profile_read": ([_S, _DP], C.c_int),
+    "dimgpu_kernel_launches": ([], C.c_longlong),
     "dimgpu_compute_dt_cfl_noalloc": ([_D, _DP, C.c_double, C.c_double, _DP, C.c_void_p], C.c_int),
     "dimgpu_batch_create": ([C.c_int, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "dimgpu_batch_destroy": ([C.c_void_p], C.c_int),

@@ -271,3 +271,84 @@ def batch_instances(n: int = 256, seed: int = 0, side_range=(64, 1024)):
         else:
             out.append(single_bubble_2d(N, seed=s))
     return out
+
+
+# ---- the single-material Euler step (model MODEL_EULER) -------------------------
+#
+# SoA components rho, mom[0..dim-1], E.  Shapes follow the sharp-interface
+# solver's single-material validation precedents (shock tubes, blast waves);
+# values are drawn per seed.
+
+def euler_prim_to_cons(dim: int, kind: str, gamma: float, p_inf: float, rho, vel, p) -> np.ndarray:
+    """prim_to_cons of the Euler step (src/euler/primitives.hpp:7-34), vectorised,
+    for building initial fields only."""
+    rho = np.asarray(rho, dtype=np.float64)
+    n = rho.shape[0]
+    out = np.empty((dim + 2, n))
+    out[0] = rho
+    out[1:1 + dim] = rho * vel
+    e = (p + (gamma * p_inf if kind == "stiffened_gas" else 0.0)) / ((gamma - 1.0) * rho)
+    out[1 + dim] = rho * e + 0.5 * rho * (vel * vel).sum(axis=0)
+    return out
+
+
+def euler_tube(seed: int = 0, N=(1000,), axis: int = 0, position: float = 0.5, material=None,
+               bc=None, time_update: str = "split") -> tuple[Desc, np.ndarray]:
+    """Single-material Riemann tube along `axis`: left / right states drawn
+    per seed (rho log-U[0.1, 10] ideal, log-U[100, 1000] stiffened; p
+    log-U[1e4, 1e7]; u U[-50, 50]), or Sod's tube for seed < 0."""
+    dim = len(N)
+    rng = np.random.default_rng(seed if seed >= 0 else 0)
+    if material is None:
+        material = ("ideal_gas", 1.4, 0.0) if seed < 0 or seed % 3 != 2 else ("stiffened_gas", 4.4, 6e8)
+    kind, gamma, p_inf = material
+    if seed < 0:
+        left, right = (1.0, 0.0, 1.0), (0.125, 0.0, 0.1)
+    else:
+        def side():
+            if kind == "stiffened_gas":
+                rho = math.exp(rng.uniform(math.log(100.0), math.log(1000.0)))
+            else:
+                rho = math.exp(rng.uniform(math.log(0.1), math.log(10.0)))
+            return rho, rng.uniform(-50.0, 50.0), math.exp(rng.uniform(math.log(1e4), math.log(1e7)))
+        left, right = side(), side()
+    lengths = [1.0] * dim
+    dx = [lengths[a] / N[a] for a in range(dim)]
+    bc = bc or ["transmissive"] * dim
+    d = make_desc(dim, N, dx, [material], bc_lo=bc, bc_hi=bc, time_update=time_update, model=1)
+    n = int(np.prod(N))
+    idx = np.unravel_index(np.arange(n), tuple(reversed(N)))
+    coord = (idx[dim - 1 - axis] + 0.5) * dx[axis]
+    is_left = coord < position * lengths[axis]
+    rho = np.where(is_left, left[0], right[0])
+    vel = np.zeros((dim, n))
+    vel[axis] = np.where(is_left, left[1], right[1])
+    p = np.where(is_left, left[2], right[2])
+    return d, np.ascontiguousarray(euler_prim_to_cons(dim, kind, gamma, p_inf, rho, vel, p))
+
+
+def euler_blast(N=(256, 256), seed: int = 0, material=("ideal_gas", 1.4, 0.0), bc=None,
+                time_update: str = "split") -> tuple[Desc, np.ndarray]:
+    """Blast wave: a high-pressure sphere (circle) of radius 0.1 at a seeded
+    centre near the middle of the unit box, ambient rho = 1, p = 1e5 (1e5
+    ambient, 1e9 inside for stiffened water), with seeded small velocity
+    noise so no axis is symmetric."""
+    dim = len(N)
+    rng = np.random.default_rng(seed)
+    kind, gamma, p_inf = material
+    dx = [1.0 / N[a] for a in range(dim)]
+    bc = bc or ["transmissive"] * dim
+    d = make_desc(dim, N, dx, [material], bc_lo=bc, bc_hi=bc, time_update=time_update, model=1)
+    n = int(np.prod(N))
+    idx = np.unravel_index(np.arange(n), tuple(reversed(N)))
+    centre = 0.5 + rng.uniform(-0.05, 0.05, size=dim)
+    r2 = np.zeros(n)
+    for a in range(dim):
+        x = (idx[dim - 1 - a] + 0.5) * dx[a]
+        r2 += (x - centre[a]) ** 2
+    inside = r2 < 0.1 ** 2
+    stiff = kind == "stiffened_gas"
+    rho = np.where(inside, 1200.0 if stiff else 1.0, 1000.0 if stiff else 0.125)
+    p = np.where(inside, 1e9 if stiff else 1e6, 1e5)
+    vel = rng.uniform(-1.0, 1.0, size=(dim, n))
+    return d, np.ascontiguousarray(euler_prim_to_cons(dim, kind, gamma, p_inf, rho, vel, p))

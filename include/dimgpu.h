@@ -96,6 +96,16 @@ enum {
     DIMGPU_TIME_UNSPLIT = 1
 };
 
+/* Which step a session runs. */
+enum {
+    DIMGPU_MODEL_DIM = 0,   /* dim::advance_one_step (src/dim/solver/advance_step.hpp:150) */
+    DIMGPU_MODEL_EULER = 1  /* the single-material Euler step: advance_one_step<DIM, EOS>
+                             * (src/sim/solver/advance_step.hpp:489) with one material
+                             * and no level set; nmat = 1, V = 2 + DIM components
+                             * (rho, mom[0..DIM-1], E: Conserved<DIM>,
+                             * src/euler/state.hpp:8-12), every axis N >= 3 */
+};
+
 /* One material: the fields of ::EOSParams that the ideal and stiffened-gas
  * laws read (src/euler/eos_params.hpp:46-53). */
 typedef struct dimgpu_material {
@@ -118,6 +128,7 @@ typedef struct dimgpu_desc {
     double alpha_source_floor;      /* Config::dim_alpha_source_floor             */
     int precision;                  /* DIMGPU_PRECISION_*                         */
     int time_update;                /* DIMGPU_TIME_*                              */
+    int model;                      /* DIMGPU_MODEL_* (0: DIM)                    */
 } dimgpu_desc;
 
 /* Per-call phase timings, the device-side counterpart of SolverPhaseTimings
@@ -221,6 +232,11 @@ int dimgpu_set_schedule(dimgpu_session* s, int dir, int schedule);
  * (8 doubles), accumulated since profiling was last enabled. */
 int dimgpu_profile(dimgpu_session* s, int enable);
 int dimgpu_profile_read(dimgpu_session* s, double* out8);
+
+/* Kernels this library has launched in the process so far (all sessions and
+ * batches; a batch step replayed from a CUDA graph counts the kernels the
+ * graph holds for it).  The difference of two reads brackets a region. */
+long long dimgpu_kernel_launches(void);
 
 /* CFL time step of a state that the caller keeps in its own device memory,
  * computed without allocating anything.  No counterpart in the reference: it

@@ -154,3 +154,78 @@ def reference() -> Checker:
 
 def reference_available() -> bool:
     return os.path.exists(REF_SO)
+
+
+EREF_SO = os.path.join(HERE, "_ref", "libeulerref.so")
+
+
+class EulerChecker:
+    """The single-material Euler step: ``port`` (oracle/euler_oracle.c, in
+    libdimoracle.so) or ``reference`` (oracle/_ref/libeulerref.so, the
+    reference's own advance_one_step<DIM, MaterialEOS> with no level set).
+    SoA state: rho, mom[0..dim-1], E per cell."""
+
+    def __init__(self, kind: str = "port"):
+        self.kind = kind
+        path = PORT_SO if kind == "port" else EREF_SO
+        if not os.path.exists(path):
+            raise FileNotFoundError(f"{kind} Euler checker not built: {path}")
+        self.lib = C.CDLL(path)
+        self.prefix = "euler_oracle_" if kind == "port" else "eref_"
+
+    def _fn(self, name):
+        f = getattr(self.lib, self.prefix + name)
+        f.restype = C.c_int
+        return f
+
+    def _check(self, rc, name):
+        if rc != 0:
+            msg = ""
+            if self.kind == "reference":
+                f = self.lib.eref_last_error
+                f.restype = C.c_char_p
+                msg = f().decode()
+            raise RuntimeError(f"euler {self.kind}.{name}: status {rc} {msg}")
+
+    def set_threads(self, n: int) -> None:
+        if self.kind == "reference":
+            self.lib.eref_set_threads(C.c_int(n))
+
+    def advance(self, d: Desc, soa: np.ndarray, cfl: float, dt_max: float, nsteps: int = 1):
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        out = np.empty_like(soa)
+        dts = np.zeros(max(nsteps, 1))
+        rc = self._fn("advance")(C.byref(d), dptr(soa), dptr(out), C.c_double(cfl), C.c_double(dt_max),
+                                 C.c_int(nsteps), dptr(dts))
+        self._check(rc, "advance")
+        return out, dts[:nsteps]
+
+    def compute_dt_cfl(self, d: Desc, soa: np.ndarray, cfl: float, dt_max: float) -> float:
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        dt = C.c_double(0.0)
+        rc = self._fn("compute_dt_cfl")(C.byref(d), dptr(soa), C.c_double(cfl), C.c_double(dt_max), C.byref(dt))
+        self._check(rc, "compute_dt_cfl")
+        return dt.value
+
+    def hllc(self, d: Desc, direction: int, UL: np.ndarray, UR: np.ndarray) -> np.ndarray:
+        """Rows of (rho, mom, E) face states -> rows of fluxes."""
+        UL = np.ascontiguousarray(UL, dtype=np.float64)
+        UR = np.ascontiguousarray(UR, dtype=np.float64)
+        out = np.empty_like(UL)
+        rc = self._fn("hllc")(C.byref(d), C.c_int(len(UL)), C.c_int(direction), dptr(UL), dptr(UR), dptr(out))
+        self._check(rc, "hllc")
+        return out
+
+    # port only: the sub-calls of one step
+    def sweep_direction(self, d: Desc, direction: int, dt: float, soa: np.ndarray, out: np.ndarray | None = None):
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        out = np.zeros_like(soa) if out is None else np.ascontiguousarray(out, dtype=np.float64).copy()
+        rc = self.lib.euler_oracle_sweep_direction(C.byref(d), C.c_int(direction), C.c_double(dt), dptr(soa),
+                                                   dptr(out))
+        self._check(rc, "sweep_direction")
+        return out
+
+    def apply_boundary_conditions(self, d: Desc, soa: np.ndarray) -> np.ndarray:
+        out = np.ascontiguousarray(soa, dtype=np.float64).copy()
+        self._check(self.lib.euler_oracle_apply_boundary_conditions(C.byref(d), dptr(out)), "boundary")
+        return out

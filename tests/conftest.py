@@ -24,7 +24,8 @@ def build_host_harness() -> str:
     """g++ build of the device arithmetic for the host (tests/native)."""
     src = os.path.join(ROOT, "tests", "native", "physics_host.cpp")
     csrc = os.path.join(ROOT, "diffuse_vs_gfm_mms_b200", "csrc")
-    deps = [src] + [os.path.join(csrc, h) for h in ("dim_physics.h", "dim_line.h")]
+    deps = [src] + [os.path.join(csrc, h) for h in ("dim_physics.h", "dim_line.h", "dim_mixed.h",
+                                                                "euler_physics.h")]
     if os.path.exists(HOST_SO) and os.path.getmtime(HOST_SO) >= max(os.path.getmtime(p) for p in deps):
         return HOST_SO
     os.makedirs(os.path.dirname(HOST_SO), exist_ok=True)
@@ -48,3 +49,19 @@ def reference():
     if not O.reference_available():
         pytest.skip("reference build (oracle/_ref) absent")
     return O.reference()
+
+
+@pytest.fixture(scope="session")
+def euler_port():
+    from oracle import oracle as O
+    if not os.path.exists(O.PORT_SO):
+        O.build()
+    return O.EulerChecker("port")
+
+
+@pytest.fixture(scope="session")
+def euler_reference():
+    from oracle import oracle as O
+    if not os.path.exists(O.EREF_SO):
+        pytest.skip("reference Euler build (oracle/_ref/libeulerref.so) absent")
+    return O.EulerChecker("reference")

@@ -2,7 +2,8 @@
 
     make -C oracle && python tests/golden/make_golden.py
 
-Runs oracle/_ref/libdimref.so — the reference's own header-only DIM code
+Runs oracle/_ref/libdimref.so and oracle/_ref/libeulerref.so — the
+reference's own header-only DIM step and single-material Euler step,
 compiled from its sources by oracle/Makefile — on seeded inputs and stores
 inputs and outputs as .npz fixtures.  The reference publishes no numeric
 golden vectors of its own, so these pin the CPU restatement (and, through it,
@@ -109,12 +110,62 @@ def field_cases(ref: O.Checker):
     return out
 
 
+EULER_CASES = {
+    "sod_200": (lambda: W.euler_tube(seed=-1, N=(200,)), 0.8, 30),
+    "tube_300_s0": (lambda: W.euler_tube(seed=0, N=(300,)), 0.8, 30),
+    "tube_water_300": (lambda: W.euler_tube(seed=2, N=(300,)), 0.8, 30),
+    "tube_2d_y": (lambda: W.euler_tube(seed=1, N=(12, 64), axis=1), 0.6, 20),
+    "blast_2d": (lambda: W.euler_blast(N=(40, 36), seed=3), 0.6, 20),
+    "blast_2d_reflective": (lambda: W.euler_blast(N=(36, 32), seed=4, bc=["reflective", "reflective"]), 0.6, 20),
+    "blast_2d_nonreflective": (lambda: W.euler_blast(N=(36, 32), seed=5, bc=["nonreflective", "transmissive"]),
+                               0.6, 20),
+    "blast_2d_water": (lambda: W.euler_blast(N=(32, 32), seed=6, material=("stiffened_gas", 4.4, 6e8)), 0.6, 20),
+    "blast_2d_unsplit": (lambda: W.euler_blast(N=(32, 30), seed=7, time_update="unsplit"), 0.5, 20),
+    "blast_3d": (lambda: W.euler_blast(N=(14, 12, 10), seed=8), 0.6, 10),
+    "nonreflective_n3": (lambda: W.euler_blast(N=(3, 24), seed=9, bc=["nonreflective", "nonreflective"]), 0.5, 10),
+}
+
+
+def euler_cases(eref: O.EulerChecker):
+    """The single-material Euler step (oracle/_ref/libeulerref.so)."""
+    out = {}
+    for name, (gen, cfl, n) in EULER_CASES.items():
+        d, U = gen()
+        outU, dts = eref.advance(d, U, cfl, 1e300, n)
+        out[f"{name}_desc"] = desc_to_array(d)
+        out[f"{name}_in"] = U
+        out[f"{name}_out"] = outU
+        out[f"{name}_dt"] = dts
+        out[f"{name}_meta"] = np.array([cfl, n])
+    # HLLC records on random face pairs (ideal and stiffened), both axes of 2D
+    for tag, mat in (("ideal", ("ideal_gas", 1.4, 0.0)), ("water", ("stiffened_gas", 4.4, 6e8))):
+        d = abi.make_desc(2, [4, 4], [0.1, 0.1], [mat], model=abi.MODEL_EULER)
+        rng = np.random.default_rng(11 if tag == "ideal" else 12)
+        n = 200
+        rho = np.exp(rng.uniform(np.log(0.1), np.log(1000.0), size=(2, n)))
+        vel = rng.uniform(-300.0, 300.0, size=(2, 2, n))
+        p = np.exp(rng.uniform(np.log(1e3), np.log(1e9), size=(2, n)))
+        UL = W.euler_prim_to_cons(2, mat[0], mat[1], mat[2], rho[0], vel[0], p[0]).T.copy()
+        UR = W.euler_prim_to_cons(2, mat[0], mat[1], mat[2], rho[1], vel[1], p[1]).T.copy()
+        out[f"hllc_{tag}_desc"] = desc_to_array(d)
+        out[f"hllc_{tag}_UL"] = UL
+        out[f"hllc_{tag}_UR"] = UR
+        for axis in (0, 1):
+            out[f"hllc_{tag}_F{axis}"] = eref.hllc(d, axis, UL, UR)
+    return out
+
+
 def main():
-    if not O.reference_available():
-        raise SystemExit("oracle/_ref/libdimref.so missing: run make -C oracle where the reference sources exist")
-    ref = O.reference()
-    np.savez_compressed(os.path.join(HERE, "kat_records.npz"), **kat_records(ref))
-    np.savez_compressed(os.path.join(HERE, "field_steps.npz"), **field_cases(ref))
+    """python tests/golden/make_golden.py [dim | euler | all] (default all)."""
+    which = sys.argv[1] if len(sys.argv) > 1 else "all"
+    if which in ("dim", "all"):
+        if not O.reference_available():
+            raise SystemExit("oracle/_ref/libdimref.so missing: run make -C oracle where the reference sources exist")
+        ref = O.reference()
+        np.savez_compressed(os.path.join(HERE, "kat_records.npz"), **kat_records(ref))
+        np.savez_compressed(os.path.join(HERE, "field_steps.npz"), **field_cases(ref))
+    if which in ("euler", "all"):
+        np.savez_compressed(os.path.join(HERE, "euler_steps.npz"), **euler_cases(O.EulerChecker("reference")))
     print("wrote", os.listdir(HERE))
 
 

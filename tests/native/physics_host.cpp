@@ -8,6 +8,8 @@
 #include <vector>
 
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_line.h"
+#include "../../diffuse_vs_gfm_mms_b200/csrc/dim_mixed.h"
+#include "../../diffuse_vs_gfm_mms_b200/csrc/euler_physics.h"
 #include "dimgpu.h"
 
 using namespace dimgpu;
@@ -103,6 +105,153 @@ int solve_line_stages(const Mats& M, int n, const State<NM, D>* U, State<NM, D>*
     return 0;
 }
 
+// The mixed-precision line schedule (stage A, stage_b_mixed, face_mixed +
+// stage_d_mixed, stage E), untiled.
+template<int NM, int D>
+int solve_line_mixed(const Mats& M, int n, const State<NM, D>* U, State<NM, D>* out, int dir, double dt, double dx)
+{
+    if (n == 1) {
+        out[0] = U[0];
+        return 0;
+    }
+    std::vector<CellA<NM, D>> A(n);
+    std::vector<Prim<NM, D>> Ph(n);
+    std::vector<FaceD<NM, D>> F(n);
+    auto is_end = [&](int i) { return i == 0 || i == n - 1 || n < 3; };
+    for (int i = 0; i < n; ++i) stage_a<NM, D>(M, U[i], A[i]);
+    for (int i = 0; i < n; ++i) {
+        const Prim<NM, D>& lo = A[i > 0 ? i - 1 : i].Pe;
+        const Prim<NM, D>& hi = A[i < n - 1 ? i + 1 : i].Pe;
+        stage_b_mixed<NM, D>(M, U[i], A[i], lo, hi, is_end(i), dir, dt, dx, Ph[i]);
+    }
+    for (int i = 0; i + 1 < n; ++i) {
+        State<NM, D> UL, UR;
+        Prim<NM, D> PL, PR;
+        if (is_end(i)) { UL = U[i]; PL = A[i].P; }
+        else face_mixed<NM, D>(M, Ph[i - 1], Ph[i], Ph[i + 1], true, UL, PL);
+        if (is_end(i + 1)) { UR = U[i + 1]; PR = A[i + 1].P; }
+        else face_mixed<NM, D>(M, Ph[i], Ph[i + 1], Ph[i + 2], false, UR, PR);
+        if (!stage_d_mixed<NM, D>(M, UL, PL, UR, PR, dir, F[i])) return DIMGPU_E_NONFINITE;
+    }
+    for (int i = 0; i < n; ++i) {
+        const FaceD<NM, D>* lo = i > 0 ? &F[i - 1] : nullptr;
+        const FaceD<NM, D>* hi = i < n - 1 ? &F[i] : nullptr;
+        stage_e<NM, D>(M, U[i], A[i], lo, hi, i == 0, i == n - 1, dt, dx, out[i]);
+    }
+    return 0;
+}
+
+
+// The Euler sweep of one line through the device stages of euler_physics.h
+// (the order euler_sweep_kernel evaluates them), untiled.
+template<int D>
+int euler_line(const Mats& M, int n, const EState<D>* U, EState<D>* out, int dir, double dt, double dx,
+               int ends_copy)
+{
+    std::vector<EPrim<D>> P(n), Ph(n);
+    std::vector<EState<D>> LS(n), RS(n), F(n);
+    bool ok = true;
+    for (int i = 0; i < n; ++i) {
+        P[i] = e_cons_to_prim<D>(M, U[i]);
+        e_enforce_prim<D>(P[i]);
+    }
+    for (int i = 0; i < n; ++i) {
+        if (i == 0 || i == n - 1) { Ph[i] = P[i]; continue; }
+        const EState<D> Ul = e_face_state<D>(M, P[i - 1], P[i], P[i + 1], false);
+        const EState<D> Ur = e_face_state<D>(M, P[i - 1], P[i], P[i + 1], true);
+        EState<D> Uh;
+        ok &= e_hancock<D>(M, U[i], Ul, Ur, dir, dt, dx, Uh);
+        Ph[i] = e_cons_to_prim<D>(M, Uh);
+        e_enforce_prim<D>(Ph[i]);
+    }
+    for (int i = 0; i < n; ++i) {
+        if (i == 0 || i == n - 1) { LS[i] = U[i]; RS[i] = U[i]; }
+        else {
+            LS[i] = e_face_state<D>(M, Ph[i - 1], Ph[i], Ph[i + 1], false);
+            RS[i] = e_face_state<D>(M, Ph[i - 1], Ph[i], Ph[i + 1], true);
+        }
+        e_enforce<D>(M, LS[i]);
+        e_enforce<D>(M, RS[i]);
+    }
+    for (int i = 0; i + 1 < n; ++i) ok &= e_hllc<D>(M, RS[i], LS[i + 1], dir, F[i]);
+    for (int i = 0; i < n; ++i) {
+        if (i == 0 || i == n - 1) {
+            if (ends_copy) out[i] = U[i];
+            else {
+                out[i].rho = 0.0;
+                for (int d = 0; d < D; ++d) out[i].mom[d] = 0.0;
+                out[i].E = 0.0;
+            }
+            continue;
+        }
+        e_update<D>(M, U[i], F[i - 1], F[i], dt, dx, out[i]);
+    }
+    return ok ? 0 : DIMGPU_E_NONFINITE;
+}
+
+template<int D>
+int euler_sweep_impl(const dimgpu_desc* d, int dir, double dt, const double* in, double* out, int ends_copy)
+{
+    const Mats M = mats_of(d);
+    size_t total = 1, stride[3] = {1, 1, 1};
+    for (int a = 0; a < D; ++a) total *= (size_t)d->N[a];
+    for (int a = 1; a < D; ++a) stride[a] = stride[a - 1] * (size_t)d->N[a - 1];
+    const int n = d->N[dir];
+    const size_t lines = total / (size_t)n;
+    int rc = 0;
+    std::vector<EState<D>> lin(n), lout(n);
+    for (size_t line = 0; line < lines; ++line) {
+        int idx[3] = {0, 0, 0};
+        size_t tmp = line;
+        for (int a = D - 1; a >= 0; --a) {
+            if (a == dir) continue;
+            idx[a] = (int)(tmp % (size_t)d->N[a]);
+            tmp /= (size_t)d->N[a];
+        }
+        size_t base = 0;
+        for (int a = 0; a < D; ++a) base += (size_t)idx[a] * stride[a];
+        for (int i = 0; i < n; ++i) {
+            const size_t c = base + (size_t)i * stride[dir];
+            lin[i].rho = in[c];
+            for (int a = 0; a < D; ++a) lin[i].mom[a] = in[(1 + a) * total + c];
+            lin[i].E = in[(1 + D) * total + c];
+        }
+        const int r = euler_line<D>(M, n, lin.data(), lout.data(), dir, dt, d->dx[dir], ends_copy);
+        if (r) rc = r;
+        for (int i = 0; i < n; ++i) {
+            const size_t c = base + (size_t)i * stride[dir];
+            out[c] = lout[i].rho;
+            for (int a = 0; a < D; ++a) out[(1 + a) * total + c] = lout[i].mom[a];
+            out[(1 + D) * total + c] = lout[i].E;
+        }
+    }
+    return rc;
+}
+
+template<int D>
+int euler_hllc_impl(const dimgpu_desc* d, int n, int dir, const double* UL, const double* UR, double* out)
+{
+    const Mats M = mats_of(d);
+    const int V = 2 + D;
+    int rc = 0;
+    for (int i = 0; i < n; ++i) {
+        EState<D> a, b, F;
+        a.rho = UL[i * V];
+        b.rho = UR[i * V];
+        for (int k = 0; k < D; ++k) {
+            a.mom[k] = UL[i * V + 1 + k];
+            b.mom[k] = UR[i * V + 1 + k];
+        }
+        a.E = UL[i * V + 1 + D];
+        b.E = UR[i * V + 1 + D];
+        if (!e_hllc<D>(M, a, b, dir, F)) { rc = DIMGPU_E_NONFINITE; continue; }
+        out[i * V] = F.rho;
+        for (int k = 0; k < D; ++k) out[i * V + 1 + k] = F.mom[k];
+        out[i * V + 1 + D] = F.E;
+    }
+    return rc;
+}
+
 template<int NM, int D>
 int sweep_impl(const dimgpu_desc* d, int dir, double dt, const double* in, double* out)
 {
@@ -125,7 +274,9 @@ int sweep_impl(const dimgpu_desc* d, int dir, double dt, const double* in, doubl
         size_t base = 0;
         for (int a = 0; a < D; ++a) base += (size_t)idx[a] * stride[a];
         for (int i = 0; i < n; ++i) load<NM, D>(in + base + (size_t)i * stride[dir], lin[i], total);
-        const int r = solve_line_stages<NM, D>(M, n, lin.data(), lout.data(), dir, dt, d->dx[dir]);
+        const int r = d->precision == DIMGPU_PRECISION_MIXED
+                          ? solve_line_mixed<NM, D>(M, n, lin.data(), lout.data(), dir, dt, d->dx[dir])
+                          : solve_line_stages<NM, D>(M, n, lin.data(), lout.data(), dir, dt, d->dx[dir]);
         if (r) rc = r;
         for (int i = 0; i < n; ++i) store<NM, D>(out + base + (size_t)i * stride[dir], lout[i], total);
     }
@@ -280,6 +431,25 @@ int host_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, const doub
 int host_solve_line(const dimgpu_desc* d, int n, int dir, double dt, double dx, const double* in, double* out)
 {
     DISPATCH(d, line_impl, d, n, dir, dt, dx, in, out);
+}
+int host_euler_sweep_direction(const dimgpu_desc* d, int dir, double dt, const double* in, double* out,
+                               int ends_copy)
+{
+    switch (d->dim) {
+        case 1: return euler_sweep_impl<1>(d, dir, dt, in, out, ends_copy);
+        case 2: return euler_sweep_impl<2>(d, dir, dt, in, out, ends_copy);
+        case 3: return euler_sweep_impl<3>(d, dir, dt, in, out, ends_copy);
+        default: return DIMGPU_E_INVALID_ARG;
+    }
+}
+int host_euler_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, const double* UR, double* out)
+{
+    switch (d->dim) {
+        case 1: return euler_hllc_impl<1>(d, n, dir, UL, UR, out);
+        case 2: return euler_hllc_impl<2>(d, n, dir, UL, UR, out);
+        case 3: return euler_hllc_impl<3>(d, n, dir, UL, UR, out);
+        default: return DIMGPU_E_INVALID_ARG;
+    }
 }
 int host_sweep_direction(const dimgpu_desc* d, int dir, double dt, const double* in, double* out)
 {

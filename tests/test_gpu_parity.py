@@ -246,3 +246,20 @@ def test_errors_are_statuses():
     bad = abi.make_desc(1, [8], [0.1], [("ideal_gas", 1.0, 0.0)])
     with pytest.raises(DimGpuError):
         Session(bad)
+
+
+def test_autotuned_schedule_gives_the_same_result(tmp_path, monkeypatch):
+    from diffuse_vs_gfm_mms_b200 import autotune
+    monkeypatch.setenv("DIMGPU_TUNE_CACHE", str(tmp_path / "tune.json"))
+    d, U = W.bubble_cloud_3d(N=(48, 40, 36), nbubbles=4)
+    choice = autotune.tune(d, U, cfl=0.6, repeats=1, force=True)
+    assert set(choice) == {0, 1, 2}
+    assert autotune.tune(d, U, cfl=0.6) == choice          # served from the cache
+    with Session(d, U) as s:
+        autotune.apply(s, choice)
+        s.steps(3, 0.6, 1e300)
+        tuned = s.download()
+    with Session(d, U) as s:
+        s.steps(3, 0.6, 1e300)
+        plain = s.download()
+    assert ndiff(tuned, plain) == 0
