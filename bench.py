@@ -1,6 +1,6 @@
 """Benchmark of the B200 DIM step (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c0]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c1|c2|c0|c3|c4|e2|e3]
     python bench.py --impl reference ...      # the reference's own CPU code
 
 A step is one DIM time step (CFL reduction, one split sweep per axis, a
@@ -9,7 +9,11 @@ boundary fill after each) over the whole grid of the workload:
   c1  2D shock-bubble, 1024x512, two materials (the default: the metric's
       configuration that fits one GPU);
   c2  3D bubble cloud, 512^3, two materials;
-  c0  1D two-material Riemann tube, 1000 cells.
+  c0  1D two-material Riemann tube, 1000 cells;
+  c3  256 uneven 2D instances in one persistent batch (solves/s);
+  c4  the serving loop (p50 / p99 latency, solves/s);
+  e2  single-material Euler step (the sharp-interface solver's no-level-set
+      path), 2D blast 2048x2048;  e3  the same, 3D 256^3.
 
 value  = cell updates per second with the state resident in HBM (CUDA events
          on the session's stream, one event pair per step; the L2 is flushed
@@ -49,7 +53,10 @@ WORKLOADS = {
     "c4": ("Poisson stream of DIM requests: 40% 1D N in [256,8192], 60% 2D sides in [128,2048], "
            "steps in [100,2000], 150 GB budget", 0.6),
     "c3": ("256 independent 2D instances, sides log-uniform in [64,1024], Riemann or bubble, CFL 0.6", 0.6),
+    "e2": ("single-material Euler step (no level set): 2D blast 2048x2048, ideal gas, CFL 0.6", 0.6),
+    "e3": ("single-material Euler step (no level set): 3D blast 256^3, ideal gas, CFL 0.6", 0.6),
 }
+EULER_WORKLOADS = ("e2", "e3")
 
 
 def make_workload(name: str, scale: int = 1):
@@ -61,6 +68,10 @@ def make_workload(name: str, scale: int = 1):
         return W.bubble_cloud_3d(N=(n, n, n), nbubbles=64)
     if name == "c0":
         return W.riemann(seed=0, N=(1000,))
+    if name == "e2":
+        return W.euler_blast(N=(2048 // scale, 2048 // scale), seed=0)
+    if name == "e3":
+        return W.euler_blast(N=(256 // scale,) * 3, seed=0)
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -79,6 +90,18 @@ def reference_sample(name: str):
         d, U = W.bubble_cloud_3d(N=(64, 64, 64), nbubbles=64)
         d.dx[0] = d.dx[1] = d.dx[2] = 1.0 / 512
         return d, U, "64^3 block of the 512^3 case (same spacing, 64 bubbles)"
+    if name in ("e2", "e3"):
+        d, U = make_workload(name)
+        V = d.nvar
+        if name == "e2":
+            U3 = U.reshape(V, 2048, 2048)[:, 992:1056, :]
+            d2 = d.copy()
+            d2.N[1] = 64
+            return d2, np.ascontiguousarray(U3.reshape(V, -1)), "2048x64 strip through the blast centre"
+        U4 = U.reshape(V, 256, 256, 256)[:, 112:144, :, :]
+        d2 = d.copy()
+        d2.N[2] = 32
+        return d2, np.ascontiguousarray(U4.reshape(V, -1)), "256x256x32 slab through the blast centre"
     d, U = W.riemann(seed=0, N=(1000,))
     return d, U, "the whole 1000-cell tube"
 
@@ -176,8 +199,12 @@ def cpu_reference_rate(workload: str, steps: int, warmup: int):
     os.environ.setdefault("OMP_SCHEDULE", "guided,1")
     os.environ.setdefault("OMP_DYNAMIC", "FALSE")
     from oracle import oracle as O
-    kind = "reference" if O.reference_available() else "port"
-    chk = O.reference() if kind == "reference" else O.port()
+    if workload in EULER_WORKLOADS:
+        kind = "reference" if os.path.exists(O.EREF_SO) else "port"
+        chk = O.EulerChecker(kind)
+    else:
+        kind = "reference" if O.reference_available() else "port"
+        chk = O.reference() if kind == "reference" else O.port()
     chk.set_threads(nthreads)
     d, U, sample = reference_sample(workload)
     cfl = WORKLOADS[workload][1]
@@ -187,7 +214,8 @@ def cpu_reference_rate(workload: str, steps: int, warmup: int):
     chk.advance(d, U, cfl, 1e300, steps)
     el = time.perf_counter() - t0
     rate = d.ncell * steps / el
-    return {"value": rate, "unit": UNIT, "cores": chk.max_threads(), "kind": kind,
+    cores = chk.max_threads() if hasattr(chk, "max_threads") else (nthreads if kind == "reference" else 1)
+    return {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
             "sample": f"{sample}; {steps} steps after {warmup} warm-up", "seconds": el}
 
 
@@ -336,6 +364,8 @@ def run_ours(args):
     traffic, traffic_src = ncu_traffic(args.workload + ("-mixed" if args.precision == "mixed" else ""))
     sched = "mixed staged sweep (staged_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
         "staged sweep (staged_a..staged_e)"
+    if args.workload in EULER_WORKLOADS:
+        sched = "euler_sweep_kernel (fused tile)"
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,

@@ -235,15 +235,21 @@ DHD bool e_hllc(const Mats& M, const EState<D>& UL, const EState<D>& UR, int dir
         rhoR_star * (safe_div(UR.E, rhoR) + (s_star - unR) * (s_star + safe_div(pR, rhoR * (sR - unR))));
     if (!fin(rhoL_star) || !fin(EL_star) || rhoL_star <= 0.0) return false;
     if (!fin(rhoR_star) || !fin(ER_star) || rhoR_star <= 0.0) return false;
-    EState<D> FK;
+    // Region selection (hllc.hpp:112-151).  The face values of the chosen
+    // side are picked element by element, so no array is addressed through
+    // a runtime-selected pointer (which would put the states in local memory).
     const bool useL = (0.0 <= sL) || (sL <= 0.0 && 0.0 <= s_star);
-    if (!e_flux<D>(M, useL ? UL : UR, dir, FK)) return false;
+    EState<D> UK;
+    UK.rho = useL ? UL.rho : UR.rho;
+#pragma unroll
+    for (int d = 0; d < D; ++d) UK.mom[d] = useL ? UL.mom[d] : UR.mom[d];
+    UK.E = useL ? UL.E : UR.E;
+    EState<D> FK;
+    if (!e_flux<D>(M, UK, dir, FK)) return false;
     if (0.0 <= sL) { F = FK; return true; }
     const bool left = (sL <= 0.0 && 0.0 <= s_star);
     const bool right = !left && (s_star <= 0.0 && 0.0 <= sR);
     if (!left && !right) { F = FK; return true; }
-    const EState<D>& UK = left ? UL : UR;
-    const double* vK = left ? vL : vR;
     const double rs = left ? rhoL_star : rhoR_star;
     const double Es = left ? EL_star : ER_star;
     const double sK = left ? sL : sR;
@@ -251,7 +257,7 @@ DHD bool e_hllc(const Mats& M, const EState<D>& UL, const EState<D>& UR, int dir
     F.rho = FK.rho + sK * (rs - UK.rho);
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        const double u = vK[d] + delta * (d == dir ? 1.0 : 0.0);
+        const double u = (left ? vL[d] : vR[d]) + delta * (d == dir ? 1.0 : 0.0);
         F.mom[d] = FK.mom[d] + sK * (rs * u - UK.mom[d]);
     }
     F.E = FK.E + sK * (Es - UK.E);

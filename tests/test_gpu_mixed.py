@@ -44,8 +44,22 @@ def _linf_rel(test, ref):
     return np.abs(test - ref).max(axis=1) / scale
 
 
-def _report(name, out, ref, dts, rdts):
-    l1 = rel_l1(out, ref)
+def _rel_l1_scored(out, ref, d):
+    """rel_l1, except that a momentum component which is zero in exact
+    arithmetic (the reference holds only round-off there, e.g. x momentum of
+    a y-aligned tube: 1e-9 of the y momentum) is scored against 1e-6 of the
+    largest momentum component's L1 instead of its own."""
+    ref2 = ref.reshape(ref.shape[0], -1)
+    out2 = out.reshape(ref2.shape)
+    den = np.abs(ref2).sum(axis=1)
+    mom = slice(d.nmat, d.nmat + d.dim)
+    den[mom] = np.maximum(den[mom], 1e-6 * den[mom].max())
+    den = np.where(den > 0, den, 1.0)
+    return np.abs(out2 - ref2).sum(axis=1) / den
+
+
+def _report(name, out, ref, dts, rdts, d=None):
+    l1 = rel_l1(out, ref) if d is None else _rel_l1_scored(out, ref, d)
     linf = _linf_rel(out, ref)
     print(f"\n{name}: rel L1 per variable {np.array2string(l1, precision=2)}; "
           f"rel Linf {np.array2string(linf, precision=2)}; dt rel diff {abs(dts[-1] / rdts[-1] - 1):.2e}")
@@ -70,7 +84,7 @@ def test_mixed_within_bound_on_well_conditioned_cases(port, name, gen, cfl, n):
     d, U = gen()
     out, dts = _mixed(d, U, cfl, n)
     ref, rdts = port.advance(d, U, cfl, 1e300, n)
-    l1 = _report(name, out, ref, dts, rdts)
+    l1 = _report(name, out, ref, dts, rdts, d)
     assert np.all(np.isfinite(out))
     assert np.all(l1 <= REL_L1_TOL), l1
 

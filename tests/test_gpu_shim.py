@@ -20,3 +20,16 @@ def test_reference_time_loop_with_drop_in_header():
     print(out.stdout)
     assert out.returncode == 0, out.stdout + out.stderr
     assert "identical" in out.stdout
+
+
+SM_EXE = os.path.join(os.path.dirname(EXE), "sm_shim_parity")
+
+
+@pytest.mark.skipif(not os.path.exists(SM_EXE), reason="sm_shim_parity is built only where the reference sources exist")
+def test_reference_single_material_step_with_drop_in_header():
+    """advance_one_step<DIM, EOS> (no level set, one material) against
+    dimgpu::sm_advance_one_step from include/dimgpu_sm_shim.hpp."""
+    out = subprocess.run([SM_EXE], capture_output=True, text=True, timeout=600)
+    print(out.stdout)
+    assert out.returncode == 0, out.stdout + out.stderr
+    assert "identical" in out.stdout
