@@ -1136,6 +1136,105 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
     return cudaGetLastError();
 }
 
+// ---- boundary flux integrand (compute_dim_boundary_flux,
+// src/app/io/conservation_report.hpp:253-305): per axis and transverse line,
+// area * (F(right end cell) - F(left end cell)) with the physical normal flux
+// of each end cell's own state; per-block partial sums ----------------------------
+template<int NM, int D>
+__global__ void __launch_bounds__(256) boundary_flux_kernel(const double* __restrict__ st, Grid g, Mats M,
+                                                            long long lines0, long long lines1, double area0,
+                                                            double area1, double area2,
+                                                            double* __restrict__ partial)
+{
+    constexpr int NV = NM + 1 + D + 1;
+    __shared__ double red[NV][256];
+    double acc[NV];
+#pragma unroll
+    for (int v = 0; v < NV; ++v) acc[v] = 0.0;
+    const long long total_lines = g.ncell / g.N[0] + (D > 1 ? g.ncell / g.N[1] : 0) + (D > 2 ? g.ncell / g.N[2] : 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total_lines; p += stride) {
+        int dir = 0;
+        long long line = p;
+        if (line >= lines0) {
+            line -= lines0;
+            dir = 1;
+            if (line >= lines1) {
+                line -= lines1;
+                dir = 2;
+            }
+        }
+        const double area = dir == 0 ? area0 : (dir == 1 ? area1 : area2);
+        int idx[3] = {0, 0, 0};
+        long long tmp = line;
+        for (int a = D - 1; a >= 0; --a) {
+            if (a == dir) continue;
+            idx[a] = (int)(tmp % g.N[a]);
+            tmp /= g.N[a];
+        }
+        long long base = 0;
+        for (int a = 0; a < D; ++a) base += (long long)idx[a] * g.stride[a];
+        for (int side = 1; side >= 0; --side) {  // right end first, as the reference adds it
+            const long long cell = base + (side ? (long long)(g.N[dir] - 1) * g.stride[dir] : 0);
+            State<NM, D> U;
+            Prim<NM, D> P;
+            load_cell<NM, D>(st, g.ncell, cell, U);
+            cons_to_prim<NM, D>(M, U, P);
+            Flux<NM, D> F;
+            flux_normal<NM, D>(U, P, dir, F);
+            const double scale = side ? area : -area;
+            double mass_flux = 0.0;
+#pragma unroll
+            for (int k = 0; k < NM; ++k) {
+                const double v = scale * F.m[k];
+                acc[k] += v;
+                mass_flux += v;
+            }
+            acc[NM] += mass_flux;
+#pragma unroll
+            for (int d = 0; d < D; ++d) acc[NM + 1 + d] += scale * F.mom[d];
+            acc[NM + 1 + D] += scale * F.E;
+        }
+    }
+#pragma unroll
+    for (int v = 0; v < NV; ++v) red[v][threadIdx.x] = acc[v];
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) {
+#pragma unroll
+            for (int v = 0; v < NV; ++v) red[v][threadIdx.x] += red[v][threadIdx.x + w];
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int v = 0; v < NV; ++v) partial[(long long)blockIdx.x * NV + v] = red[v][0];
+    }
+}
+
+template<int NM, int D>
+cudaError_t launch_boundary_flux(const Grid& g, const Mats& M, const double* state, double* partial, int max_blocks,
+                                 int* nblocks, cudaStream_t s)
+{
+    long long lines[3] = {0, 0, 0};
+    double area[3] = {1.0, 1.0, 1.0};
+    long long total = 0;
+    for (int a = 0; a < D; ++a) {
+        lines[a] = g.ncell / g.N[a];
+        total += lines[a];
+        for (int b = 0; b < D; ++b)
+            if (b != a) area[a] *= g.dx[b];
+    }
+    long long nb = (total + 255) / 256;
+    if (nb > max_blocks) nb = max_blocks;
+    if (nb < 1) nb = 1;
+    *nblocks = (int)nb;
+    boundary_flux_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, lines[0], lines[1], area[0], area[1],
+                                                            area[2], partial);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
 #define DIMGPU_INSTANTIATE_D(NM, D)                                                                          \
     template cudaError_t launch_sweep<NM, D>(const Grid&, const Mats&, int, Tile, const double*, double*,    \
                                              const double*, int*, cudaStream_t);                             \
@@ -1151,7 +1250,9 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
     template cudaError_t launch_accumulate<NM, D>(const Grid&, const Mats&, double*, const double*,          \
                                                   const double*, cudaStream_t);                              \
     template cudaError_t launch_totals<NM, D>(const Grid&, const double*, double, double*, int, int*,        \
-                                              cudaStream_t);
+                                              cudaStream_t);                                                 \
+    template cudaError_t launch_boundary_flux<NM, D>(const Grid&, const Mats&, const double*, double*, int,   \
+                                                     int*, cudaStream_t);
 
 #define DIMGPU_INSTANTIATE(NM)   \
     DIMGPU_INSTANTIATE_D(NM, 1)  \

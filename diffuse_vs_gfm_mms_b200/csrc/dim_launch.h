@@ -95,6 +95,12 @@ template<int NM, int D>
 cudaError_t launch_totals(const Grid& g, const double* state, double volume, double* partial,
                           int max_blocks, int* nblocks, cudaStream_t s);
 
+// Per-block partial sums of the boundary flux integrand (same layout as
+// launch_totals).
+template<int NM, int D>
+cudaError_t launch_boundary_flux(const Grid& g, const Mats& M, const double* state, double* partial, int max_blocks,
+                                 int* nblocks, cudaStream_t s);
+
 // ---- batched form (dim_batch.cuh) ----
 // One entry per instance of a batch, in device memory.
 struct BInst {

@@ -680,6 +680,30 @@ int dimgpu_totals(dimgpu_session* s, double* out)
     return DIMGPU_OK;
 }
 
+int dimgpu_boundary_flux(dimgpu_session* s, double* out)
+{
+    if (!s || !out) return fail(s ? &s->msg : nullptr, DIMGPU_E_INVALID_ARG, "null argument");
+    if (is_euler(s->desc))
+        return fail(&s->msg, DIMGPU_E_UNSUPPORTED, "dimgpu_boundary_flux: the DIM model only");
+    int nb = 1;
+    cudaError_t e = cudaSuccess;
+    DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                e = launch_boundary_flux<NM, D>(s->g, s->M, s->buf[s->cur], s->partial, kTotalsBlocks, &nb,
+                                                s->stream));
+    const int NV = s->desc.nmat + 1 + s->desc.dim + 1;
+    std::vector<double> h((size_t)nb * NV);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(h.data(), s->partial, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, s->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "dimgpu_boundary_flux");
+    for (int v = 0; v < NV; ++v) {
+        double acc = 0.0;
+        for (int b = 0; b < nb; ++b) acc += h[(size_t)b * NV + v];
+        out[v] = acc;
+    }
+    return DIMGPU_OK;
+}
+
 int dimgpu_set_stream(dimgpu_session* s, void* cuda_stream)
 {
     if (!s) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null session");

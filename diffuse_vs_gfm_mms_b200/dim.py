@@ -133,6 +133,13 @@ class Session:
         self._check(lib().dimgpu_totals(self._h, dptr(out)))
         return out
 
+    def boundary_flux(self) -> np.ndarray:
+        """The boundary flux integrand, laid out as totals()
+        (app_io::compute_dim_boundary_flux, src/app/io/conservation_report.hpp:253-305)."""
+        out = np.zeros(self.desc.nmat + self.desc.dim + 2)
+        self._check(lib().dimgpu_boundary_flux(self._h, dptr(out)))
+        return out
+
     # ---- tuning and measurement
     def set_stream(self, stream_handle: int | None) -> None:
         self._check(lib().dimgpu_set_stream(self._h, C.c_void_p(stream_handle or 0)))

@@ -31,6 +31,7 @@ SIGNATURES = {
     "dimgpu_sweep_direction": ([_S, C.c_int, C.c_double], C.c_int),
     "dimgpu_apply_boundary_conditions": ([_S], C.c_int),
     "dimgpu_totals": ([_S, _DP], C.c_int),
+    "dimgpu_boundary_flux": ([_S, _DP], C.c_int),
     "dimgpu_set_stream": ([_S, C.c_void_p], C.c_int),
     "dimgpu_set_tile": ([_S, C.c_int, C.c_int, C.c_int], C.c_int),
     "dimgpu_set_schedule": ([_S, C.c_int, C.c_int], C.c_int),

@@ -211,6 +211,14 @@ int dimgpu_apply_boundary_conditions(dimgpu_session* s);
  * so compare with a relative tolerance. */
 int dimgpu_totals(dimgpu_session* s, double* out);
 
+/* Boundary flux integrand of the resident state, the rate the conservation
+ * report integrates over time: per axis and transverse line,
+ * area * (F(last cell) - F(first cell)) with each end cell's own normal
+ * flux.  out receives nmat + dim + 2 values laid out as dimgpu_totals.
+ * Replaces app_io::compute_dim_boundary_flux
+ * (src/app/io/conservation_report.hpp:253-305); the DIM model only. */
+int dimgpu_boundary_flux(dimgpu_session* s, double* out);
+
 /* Run the session's work on a caller-owned CUDA stream (a cudaStream_t cast
  * to void*; NULL restores the session's own stream).  The caller keeps the
  * stream alive while the session uses it. */

@@ -1264,6 +1264,68 @@ static void load_prim(const ctx_t* c, const double* in, pr_t* P)
     P->p = in[q++];
 }
 
+/* compute_dim_boundary_flux + add_dim_flux_to_totals,
+ * src/app/io/conservation_report.hpp:149-167, 253-305: per axis, per
+ * transverse line (highest axis fastest), add area * F(right end cell), then
+ * -area * F(left end cell), in that order. */
+int oracle_boundary_flux(const dimgpu_desc* d, const double* soa, double* out)
+{
+    const int rc = validate(d);
+    if (rc) return rc;
+    ctx_t c;
+    make_ctx(d, &c);
+    const size_t total = field_cells(d);
+    double mm[MAXM] = {0}, mass = 0.0, mom[3] = {0}, energy = 0.0;
+    for (int dir = 0; dir < c.dim; ++dir) {
+        double area = 1.0;
+        for (int a = 0; a < c.dim; ++a)
+            if (a != dir) area *= d->dx[a];
+        long long lines = 1;
+        for (int a = 0; a < c.dim; ++a)
+            if (a != dir) lines *= d->N[a];
+        for (long long line = 0; line < lines; ++line) {
+            int idx[3] = {0, 0, 0};
+            long long tmp = line;
+            for (int a = c.dim - 1; a >= 0; --a) {
+                if (a == dir) continue;
+                idx[a] = (int)(tmp % d->N[a]);
+                tmp /= d->N[a];
+            }
+            for (int side = 1; side >= 0; --side) {
+                idx[dir] = side ? d->N[dir] - 1 : 0;
+                size_t lin = (size_t)idx[0];
+                size_t stride = (size_t)d->N[0];
+                for (int a = 1; a < c.dim; ++a) {
+                    lin += (size_t)idx[a] * stride;
+                    stride *= (size_t)d->N[a];
+                }
+                st_t U;
+                pr_t P;
+                fl_t F;
+                load_cell(&c, soa, total, lin, &U);
+                cons_to_prim(&c, &U, &P);
+                compute_flux_normal(&c, &U, &P, dir, &F);
+                const double scale = side ? area : -area;
+                double mass_flux = 0.0;
+                for (int k = 0; k < c.nmat; ++k) {
+                    const double v = scale * F.m[k];
+                    mm[k] += v;
+                    mass_flux += v;
+                }
+                mass += mass_flux;
+                energy += scale * F.E;
+                for (int a = 0; a < c.dim; ++a) mom[a] += scale * F.mom[a];
+            }
+        }
+    }
+    int q = 0;
+    for (int k = 0; k < c.nmat; ++k) out[q++] = mm[k];
+    out[q++] = mass;
+    for (int a = 0; a < c.dim; ++a) out[q++] = mom[a];
+    out[q++] = energy;
+    return 0;
+}
+
 int oracle_cons_to_prim(const dimgpu_desc* d, int n, const double* U, double* P)
 {
     const int rc = validate(d);

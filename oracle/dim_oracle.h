@@ -35,6 +35,7 @@ int oracle_compute_dt_cfl(const dimgpu_desc* d, const double* soa, double cfl, d
 int oracle_sweep_direction(const dimgpu_desc* d, int dir, double dt, const double* soa_in,
                            double* soa_out);
 int oracle_apply_boundary_conditions(const dimgpu_desc* d, double* soa);
+int oracle_boundary_flux(const dimgpu_desc* d, const double* soa, double* out);
 int oracle_totals(const dimgpu_desc* d, const double* soa, double* out);
 
 /* Per-function records (record-major, n records). */

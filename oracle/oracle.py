@@ -98,6 +98,13 @@ class Checker:
         self._check(self._fn("apply_boundary_conditions")(C.byref(d), dptr(out)), "bc")
         return out
 
+    def boundary_flux(self, d: Desc, soa) -> np.ndarray:
+        """compute_dim_boundary_flux: nmat + dim + 2 values, laid out as totals."""
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        out = np.zeros(d.nmat + d.dim + 2)
+        self._check(self._fn("boundary_flux")(C.byref(d), dptr(soa), dptr(out)), "boundary_flux")
+        return out
+
     # ---- record level (record-major arrays) ----
     def _records(self, name, d, inp, out_width, *extra):
         inp = np.ascontiguousarray(inp, dtype=np.float64)

@@ -17,6 +17,7 @@
 #include <string>
 #include <vector>
 
+#include "src/app/io/conservation_report.hpp"
 #include "src/dim/solver/advance_step.hpp"
 
 #include "dimgpu.h"
@@ -391,6 +392,21 @@ int ref_solve_line(const dimgpu_desc* d, int n, int dir, double dt, double dx,
         dim::solve_line<D>(in, out, dx, dt, params, dir, d->alpha_source_floor,
                            lambda_name(d->lambda_model));
         for (int i = 0; i < n; ++i) store_state<D>(U_out + (size_t)i * V, 1, 0, out[i], d->nmat);
+    });)
+    return 0;
+}
+
+int ref_boundary_flux(const dimgpu_desc* d, const double* soa, double* out)
+{
+    GUARD(DISPATCH_DIM(d, {
+        const auto params = make_params(d);
+        const auto U = load_field<D>(d, soa);
+        const auto t = app_io::compute_dim_boundary_flux<D>(U, grid_n<D>(d), grid_dx<D>(d), params);
+        int q = 0;
+        for (int k = 0; k < d->nmat; ++k) out[q++] = t.material_mass[k];
+        out[q++] = t.mass;
+        for (int a = 0; a < D; ++a) out[q++] = t.momentum[a];
+        out[q++] = t.energy;
     });)
     return 0;
 }

@@ -263,3 +263,20 @@ def test_autotuned_schedule_gives_the_same_result(tmp_path, monkeypatch):
         s.steps(3, 0.6, 1e300)
         plain = s.download()
     assert ndiff(tuned, plain) == 0
+
+
+@pytest.mark.parametrize("gen", [
+    lambda: W.riemann(seed=3, N=(500,)),
+    lambda: W.shock_bubble_2d(N=(160, 80)),
+    lambda: W.bubble_cloud_3d(N=(24, 20, 16), nbubbles=3),
+])
+def test_boundary_flux_matches_oracle(port, gen):
+    """The device boundary-flux integrand (parallel sums) against the
+    reference-order sums of the oracle."""
+    d, U = gen()
+    with Session(d, U) as s:
+        s.steps(3, 0.6, 1e300)
+        got = s.boundary_flux()
+        state = s.download()
+    want = port.boundary_flux(d, state)
+    np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12 * np.abs(want).max())

@@ -56,3 +56,16 @@ def test_oracle_rejects_unsupported_eos(port):
     d = abi.make_desc(1, [8], [0.1], [("tait", 7.0, 0.0)])
     with pytest.raises(RuntimeError):
         port.cons_to_prim(d, np.zeros((1, 3)))
+
+
+@pytest.mark.parametrize("gen", [
+    lambda: W.riemann(seed=3, N=(200,)),
+    lambda: W.shock_bubble_2d(N=(40, 20)),
+    lambda: W.bubble_cloud_3d(N=(10, 9, 8), nbubbles=2),
+    lambda: W.riemann(seed=7, N=(6, 14, 5), axis=1),
+])
+def test_boundary_flux_matches_reference(port, reference, gen):
+    """compute_dim_boundary_flux (src/app/io/conservation_report.hpp:253-305):
+    the restatement sums in the reference's order, so bit for bit."""
+    d, U = gen()
+    assert bitwise_equal(port.boundary_flux(d, U), reference.boundary_flux(d, U))
