@@ -46,14 +46,16 @@ def _linf_rel(test, ref):
 
 def _rel_l1_scored(out, ref, d):
     """rel_l1, except that a momentum component which is zero in exact
-    arithmetic (the reference holds only round-off there, e.g. x momentum of
-    a y-aligned tube: 1e-9 of the y momentum) is scored against 1e-6 of the
-    largest momentum component's L1 instead of its own."""
+    arithmetic (its L1 below 1e-6 of the largest momentum component's: the
+    reference holds only round-off there, e.g. x momentum of a y-aligned
+    tube, 2e-9 of the y momentum) is scored against the momentum scale, the
+    largest momentum component's L1, instead of its own."""
     ref2 = ref.reshape(ref.shape[0], -1)
     out2 = out.reshape(ref2.shape)
     den = np.abs(ref2).sum(axis=1)
     mom = slice(d.nmat, d.nmat + d.dim)
-    den[mom] = np.maximum(den[mom], 1e-6 * den[mom].max())
+    scale = den[mom].max()
+    den[mom] = np.where(den[mom] < 1e-6 * scale, scale, den[mom])
     den = np.where(den > 0, den, 1.0)
     return np.abs(out2 - ref2).sum(axis=1) / den
 
