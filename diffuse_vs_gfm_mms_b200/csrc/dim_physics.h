@@ -272,11 +272,22 @@ DNI double pressure_from_internal_energy(const Mats& M, double rho_total, double
 
     // Inside the loop lo <= mid <= hi, all finite and positive, so
     // clamp_min(mid) == max(mid, 1e-10); below P_fin the certain decisions
-    // are two compares and two selects.
+    // are two compares and two selects.  When P_lo > 1e-10 the clamp cannot
+    // change either decision (mid < 1e-10 is below P_lo clamped or not), so
+    // the dependency chain of a step is add, multiply, compare, select.
     const bool fast_loop = fast && clamp_min(hi) < P_fin;
+    const bool no_clamp = fast_loop && P_lo > 1e-10;
     for (int n = 0; n < 80; ++n) {
         const double mid = 0.5 * (lo + hi);
-        if (fast_loop) {
+        if (no_clamp) {
+            const bool up = mid > P_hi, dn = mid < P_lo;
+            if (up || dn) {
+                hi = up ? mid : hi;
+                lo = dn ? mid : lo;
+                continue;
+            }
+        }
+        else if (fast_loop) {
             const double pc = dmax(mid, 1e-10);
             const bool up = pc > P_hi, dn = pc < P_lo;
             if (up || dn) {

@@ -89,6 +89,13 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // `ends_copy` is 0 (the split update sweeps into a value-initialised buffer,
 // src/core/fv/directional_update.hpp:13-18) or their input state when it is
 // 1 (the unsplit update sweeps into a copy of the base state, :34-38).
+//
+// Every stage result goes to shared memory as soon as it is formed, so no
+// state stays in registers across a barrier (the cell state is re-read
+// through the read-only cache where a later stage needs it).  Three record
+// buffers of V = D + 2 doubles per slot: S0 holds P (A -> B), then RS
+// (C -> D); S1 holds Ph (B -> C), then the face flux F (D -> E); S2 holds LS
+// (C -> D).
 template<int D, int DIR>
 __global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                              Grid g, Mats M, int T, int W, int ntile, int ngx,
@@ -97,6 +104,9 @@ __global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __res
 {
     extern __shared__ double sm[];
     const int NT = T * W;
+    double* S0 = sm;
+    double* S1 = sm + (D + 2) * NT;
+    double* S2 = sm + 2 * (D + 2) * NT;
     const int t = threadIdx.x;
     const int n = g.N[DIR];
     const int OUT = T - 6;
@@ -135,37 +145,36 @@ __global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __res
     bool ok = true;
 
     // A: P_i = enforce(cons_to_prim(U_i))
-    EState<D> U;
-    EPrim<D> P;
     if (valid) {
+        EState<D> U;
         e_load<D>(in, g.ncell, cell, U);
-        P = e_cons_to_prim<D>(M, U);
+        EPrim<D> P = e_cons_to_prim<D>(M, U);
         e_enforce_prim<D>(P);
-        e_put<D>(sm, NT, t, P);
+        e_put<D>(S0, NT, t, P);
     }
     __syncthreads();
 
     // B: half step -> Ph_i
-    const bool needB = valid && (end || (pos >= 1 && pos <= T - 2));
-    EPrim<D> Ph;
-    if (needB) {
+    if (valid && (end || (pos >= 1 && pos <= T - 2))) {
+        EPrim<D> P, Ph;
+        e_get<D>(S0, NT, t, P);
         if (end) {
             Ph = P;
         }
         else {
             EPrim<D> lo, hi;
-            e_get<D>(sm, NT, t - s, lo);
-            e_get<D>(sm, NT, t + s, hi);
+            e_get<D>(S0, NT, t - s, lo);
+            e_get<D>(S0, NT, t + s, hi);
+            EState<D> U, Uh;
+            e_load<D>(in, g.ncell, cell, U);
             const EState<D> Ul = e_face_state<D>(M, lo, P, hi, false);
             const EState<D> Ur = e_face_state<D>(M, lo, P, hi, true);
-            EState<D> Uh;
             ok &= e_hancock<D>(M, U, Ul, Ur, DIR, dt, dx, Uh);
             Ph = e_cons_to_prim<D>(M, Uh);
             e_enforce_prim<D>(Ph);
         }
+        e_put<D>(S1, NT, t, Ph);
     }
-    __syncthreads();
-    if (needB) e_put<D>(sm, NT, t, Ph);
     __syncthreads();
 
     // C: face states of the second reconstruction, each enforced once more
@@ -175,43 +184,42 @@ __global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __res
         return v && (e || (p >= 2 && p <= T - 3));
     };
     const bool needC = needC_at(pos, gi);
-    EState<D> LS, RS;
     if (needC) {
+        EState<D> LS, RS;
         if (end) {
-            LS = U;
-            RS = U;
+            e_load<D>(in, g.ncell, cell, LS);
+            RS = LS;
         }
         else {
-            EPrim<D> lo, hi;
-            e_get<D>(sm, NT, t - s, lo);
-            e_get<D>(sm, NT, t + s, hi);
-            LS = e_face_state<D>(M, lo, Ph, hi, false);
-            RS = e_face_state<D>(M, lo, Ph, hi, true);
+            EPrim<D> lo, c, hi;
+            e_get<D>(S1, NT, t - s, lo);
+            e_get<D>(S1, NT, t, c);
+            e_get<D>(S1, NT, t + s, hi);
+            LS = e_face_state<D>(M, lo, c, hi, false);
+            RS = e_face_state<D>(M, lo, c, hi, true);
         }
         e_enforce<D>(M, LS);
         e_enforce<D>(M, RS);
+        e_put<D>(S2, NT, t, LS);
+        e_put<D>(S0, NT, t, RS);
     }
-    __syncthreads();
-    if (needC) e_put<D>(sm, NT, t, LS);
     __syncthreads();
 
     // D: face i|i+1
-    const bool needD = needC && pos + 1 <= T - 1 && gi + 1 < n && needC_at(pos + 1, gi + 1);
-    EState<D> F;
-    if (needD) {
-        EState<D> UR;
-        e_get<D>(sm, NT, t + s, UR);
-        ok &= e_hllc<D>(M, RS, UR, DIR, F);
+    if (needC && pos + 1 <= T - 1 && gi + 1 < n && needC_at(pos + 1, gi + 1)) {
+        EState<D> UL, UR, F;
+        e_get<D>(S0, NT, t, UL);
+        e_get<D>(S2, NT, t + s, UR);
+        ok &= e_hllc<D>(M, UL, UR, DIR, F);
+        e_put<D>(S1, NT, t, F);
     }
-    __syncthreads();
-    if (needD) e_put<D>(sm, NT, t, F);
     __syncthreads();
 
     // E: outputs
     if (valid && pos >= 3 && pos <= T - 4) {
         EState<D> Un;
         if (end) {
-            if (ends_copy) Un = U;
+            if (ends_copy) e_load<D>(in, g.ncell, cell, Un);
             else {
                 Un.rho = 0.0;
 #pragma unroll
@@ -220,9 +228,11 @@ __global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __res
             }
         }
         else {
-            EState<D> Flo;
-            e_get<D>(sm, NT, t - s, Flo);
-            e_update<D>(M, U, Flo, F, dt, dx, Un);
+            EState<D> U, Flo, Fhi;
+            e_load<D>(in, g.ncell, cell, U);
+            e_get<D>(S1, NT, t - s, Flo);
+            e_get<D>(S1, NT, t, Fhi);
+            e_update<D>(M, U, Flo, Fhi, dt, dx, Un);
         }
         e_store<D>(out, g.ncell, cell, Un);
     }
@@ -444,9 +454,11 @@ cudaError_t launch_euler_sweep_dir(const Grid& g, const Mats& M, Tile tile, cons
         const long long other = g.ncell / ((long long)g.N[0] * n);
         nblocks = (long long)ngx * ntile * other;
     }
-    const size_t smem = sizeof(double) * (size_t)(D + 2) * (size_t)(T * W);
-    euler_sweep_kernel<D, DIR><<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err,
-                                                                     ends_copy);
+    const size_t smem = sizeof(double) * 3 * (size_t)(D + 2) * (size_t)(T * W);
+    auto kern = euler_sweep_kernel<D, DIR>;
+    const cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (ea != cudaSuccess) return ea;
+    kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err, ends_copy);
     count_launches(1);
     return cudaGetLastError();
 }
