@@ -47,7 +47,11 @@ DHD void stage_a(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 
 // Stage B.  `end` is true for the first and last cell of the line and for
 // every cell of a line shorter than 3 (no reconstruction there,
-// muscl.hpp:213-226, 244-252, 271-272).
+// muscl.hpp:213-226, 244-252, 271-272).  hancock_predict's arithmetic
+// (muscl.hpp:143-191) is evaluated face by face: each face state is built,
+// repaired and turned into its flux before the other one, so a face state
+// is dead before the next out-of-line call (the same operations on the same
+// values; only independent work is reordered).
 template<int NM, int D>
 DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
                  const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, State<NM, D>& Uh,
@@ -58,14 +62,44 @@ DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
         Ph = A.Pe;
         return;
     }
+    double rhs[NM];
+    alpha_rhs_coefficients<NM, D>(M, A.Pe, A.ck, rhs);
     Prim<NM, D> Pl, Pr;
     reconstruct_cell_faces<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
-    State<NM, D> Ul, Ur;
-    prim_to_cons<NM, D>(M, Pl, Ul);
-    prim_to_cons<NM, D>(M, Pr, Ur);
-    repair_state<NM, D>(M, Ul);
-    repair_state<NM, D>(M, Ur);
-    hancock_predict<NM, D>(M, U, A.Pe, A.ck, Ul, Ur, Pl, Pr, dir, dt, dx, Uh);
+    Flux<NM, D> FL, FR;
+    {
+        State<NM, D> Ul;
+        prim_to_cons<NM, D>(M, Pl, Ul);
+        repair_state<NM, D>(M, Ul);
+        flux_normal<NM, D>(Ul, Pl, dir, FL);
+    }
+    {
+        State<NM, D> Ur;
+        prim_to_cons<NM, D>(M, Pr, Ur);
+        repair_state<NM, D>(M, Ur);
+        flux_normal<NM, D>(Ur, Pr, dir, FR);
+    }
+    const double factor = 0.5 * dt / dx;
+    Uh = U;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) Uh.m[k] -= factor * (FR.m[k] - FL.m[k]);
+#pragma unroll
+    for (int d = 0; d < D; ++d) Uh.mom[d] -= factor * (FR.mom[d] - FL.mom[d]);
+    Uh.E -= factor * (FR.E - FL.E);
+    const double u_left = Pl.vel[dir];
+    const double u_right = Pr.vel[dir];
+    const double div_u = (u_right - u_left) / dx;
+    double alpha_new[NM];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        alpha_new[k] = A.Pe.alpha[k];
+        alpha_new[k] -= factor * (Pr.alpha[k] * u_right - Pl.alpha[k] * u_left);
+        alpha_new[k] += 0.5 * dt * rhs[k] * div_u;
+    }
+    sanitise_alpha<NM>(alpha_new, 0.0);
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) Uh.a[k] = alpha_new[k];
+    repair_state<NM, D>(M, Uh);
     cons_to_prim<NM, D>(M, Uh, Ph);
     enforce_positive_primitive<NM, D>(Ph);
 }
@@ -133,8 +167,10 @@ DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
 #pragma unroll
     for (int d = 0; d < D; ++d) out.mom[d] -= lambda * (Fhi.F.mom[d] - Flo.F.mom[d]);
     out.E -= lambda * (Fhi.F.E - Flo.F.E);
-    repair_state<NM, D>(M, out);
 
+    // The fraction update reads only A and the faces, not the repaired
+    // state, so it is formed before the first repair: only alpha_new stays
+    // live across that call.
     double af_lo[NM], af_hi[NM];
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
@@ -152,6 +188,8 @@ DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
         alpha_new[k] += dt * rhs[k] * div_u;
     }
     sanitise_alpha<NM>(alpha_new, 0.0);
+
+    repair_state<NM, D>(M, out);
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) out.a[k] = alpha_new[k];
     repair_state<NM, D>(M, out);

@@ -97,7 +97,7 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // (C -> D); S1 holds Ph (B -> C), then the face flux F (D -> E); S2 holds LS
 // (C -> D).
 template<int D, int DIR>
-__global__ void __launch_bounds__(256, 2) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
+__global__ void __launch_bounds__(256, 3) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                              Grid g, Mats M, int T, int W, int ntile, int ngx,
                                                              const double* __restrict__ dtp, int* __restrict__ err,
                                                              int ends_copy)
