@@ -152,8 +152,13 @@ __global__ void __launch_bounds__(256) batch_b(const BInst* __restrict__ tab, co
         Prim<NM, D> lo, hi;
         g_get<NM, D>(b.Pe, b.cap, q - it.s, lo);
         g_get<NM, D>(b.Pe, b.cap, q + it.s, hi);
-        State<NM, D> Uh;
-        stage_b<NM, D>(I.M, U, A, lo, hi, false, DIR, I.dt, I.g.dx[DIR], Uh, Ph);
+        if (I.mixed) {
+            stage_b_mixed<NM, D>(I.M, U, A, lo, hi, false, DIR, I.dt, I.g.dx[DIR], Ph);
+        }
+        else {
+            State<NM, D> Uh;
+            stage_b<NM, D>(I.M, U, A, lo, hi, false, DIR, I.dt, I.g.dx[DIR], Uh, Ph);
+        }
     }
     g_put<NM, D>(b.Ph, b.cap, q, Ph);
     BATCH_LOOP_END
@@ -164,7 +169,7 @@ __global__ void __launch_bounds__(256) batch_c(const BInst* __restrict__ tab, co
                                                int ninst, int parity, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
-    if (!I.run || n == 1) continue;
+    if (!I.run || n == 1 || I.mixed) continue;  // mixed instances build their face states in batch_d
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
     State<NM, D> LS, RS;
     Prim<NM, D> PLS, PRS;
@@ -198,12 +203,23 @@ __global__ void __launch_bounds__(256) batch_d(const BInst* __restrict__ tab, co
     if (!I.run || n == 1 || it.gi >= n - 1) continue;
     State<NM, D> UL, UR;
     Prim<NM, D> PL, PR;
-    g_get<NM, D>(b.RS, b.cap, q, UL);
-    g_get<NM, D>(b.PRS, b.cap, q, PL);
-    g_get<NM, D>(b.LS, b.cap, q + it.s, UR);
-    g_get<NM, D>(b.PLS, b.cap, q + it.s, PR);
     FaceD<NM, D> f;
-    if (!stage_d<NM, D>(I.M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    if (I.mixed) {
+        // mixed_cd: both face states from the half-step primitives
+        mixed_face<NM, D, DIR>(in, I.g, I.M, b, it, q, n, true, UL, PL);
+        StagedItem<DIR> nx = it;
+        nx.gi += 1;
+        nx.cell += I.g.stride[DIR];
+        mixed_face<NM, D, DIR>(in, I.g, I.M, b, nx, q + it.s, n, false, UR, PR);
+        if (!stage_d_mixed<NM, D>(I.M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    }
+    else {
+        g_get<NM, D>(b.RS, b.cap, q, UL);
+        g_get<NM, D>(b.PRS, b.cap, q, PL);
+        g_get<NM, D>(b.LS, b.cap, q + it.s, UR);
+        g_get<NM, D>(b.PLS, b.cap, q + it.s, PR);
+        if (!stage_d<NM, D>(I.M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    }
     g_put<NM, D>(b.F, b.cap, q, f);
     BATCH_LOOP_END
 }

@@ -112,7 +112,7 @@ struct BInst {
     int steps_left;     // steps still to run
     int steps_done;     // steps run so far
     int run;            // runs in the current step (set by the finalize kernel)
-    int pad;
+    int mixed;          // DIMGPU_PRECISION_MIXED: mixed_b / mixed_cd arithmetic
     double cfl, dt_max;
     double dt;          // dt of the current step
 };

@@ -167,7 +167,9 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
 }
 
 // Stage B of the mixed step: FP32-limited faces, face states without the
-// repair round trip, FP64 Hancock half step and FP64 recovery into Ph.
+// repair round trip, FP64 Hancock half step (hancock_predict's arithmetic,
+// muscl.hpp:143-191, evaluated face by face as in stage_b) and FP64
+// recovery into Ph.
 template<int NM, int D>
 DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
                        const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, Prim<NM, D>& Ph)
@@ -176,13 +178,42 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
         Ph = A.Pe;
         return;
     }
+    double rhs[NM];
+    alpha_rhs_coefficients<NM, D>(M, A.Pe, A.ck, rhs);
     Prim<NM, D> Pl, Pr;
     reconstruct_mixed<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
-    State<NM, D> Ul, Ur;
-    prim_to_cons<NM, D>(M, Pl, Ul);
-    prim_to_cons<NM, D>(M, Pr, Ur);
-    State<NM, D> Uh;
-    hancock_predict<NM, D>(M, U, A.Pe, A.ck, Ul, Ur, Pl, Pr, dir, dt, dx, Uh);
+    Flux<NM, D> FL, FR;
+    {
+        State<NM, D> Ul;
+        prim_to_cons<NM, D>(M, Pl, Ul);
+        flux_normal<NM, D>(Ul, Pl, dir, FL);
+    }
+    {
+        State<NM, D> Ur;
+        prim_to_cons<NM, D>(M, Pr, Ur);
+        flux_normal<NM, D>(Ur, Pr, dir, FR);
+    }
+    const double factor = 0.5 * dt / dx;
+    State<NM, D> Uh = U;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) Uh.m[k] -= factor * (FR.m[k] - FL.m[k]);
+#pragma unroll
+    for (int d = 0; d < D; ++d) Uh.mom[d] -= factor * (FR.mom[d] - FL.mom[d]);
+    Uh.E -= factor * (FR.E - FL.E);
+    const double u_left = Pl.vel[dir];
+    const double u_right = Pr.vel[dir];
+    const double div_u = (u_right - u_left) / dx;
+    double alpha_new[NM];
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        alpha_new[k] = A.Pe.alpha[k];
+        alpha_new[k] -= factor * (Pr.alpha[k] * u_right - Pl.alpha[k] * u_left);
+        alpha_new[k] += 0.5 * dt * rhs[k] * div_u;
+    }
+    sanitise_alpha<NM>(alpha_new, 0.0);
+#pragma unroll
+    for (int k = 0; k < NM - 1; ++k) Uh.a[k] = alpha_new[k];
+    repair_state<NM, D>(M, Uh);
     cons_to_prim<NM, D>(M, Uh, Ph);
     enforce_positive_primitive<NM, D>(Ph);
 }

@@ -141,6 +141,11 @@ cudaError_t rebuild(dimgpu_batch* b)
         cells_blocks += (b->inst[i].ncell + 255) / 256;
     }
     const int nrec = staged_scratch_doubles(b->nmat, b->dim);
+    // A captured graph bakes in the launch arguments (buffer addresses and
+    // the scratch capacity that strides every record): drop it whenever any
+    // of them changes.  An address alone is not enough, since a regrown
+    // buffer can come back at the address of the one it replaces.
+    const long long caps_before[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
     const void* before[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
     cudaError_t e = grow(&b->scratch, &b->scratch_cap, std::max<long long>(items, 1) * nrec);
     if (e == cudaSuccess) e = grow(&b->blockmin, &b->blockmin_cap, std::max<long long>(cells_blocks, 1));
@@ -158,7 +163,9 @@ cudaError_t rebuild(dimgpu_batch* b)
     }
     if (e != cudaSuccess) return e;
     const void* after[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
-    if (std::memcmp(before, after, sizeof before) != 0) drop_graphs(b);
+    const long long caps_after[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
+    if (std::memcmp(before, after, sizeof before) != 0 || std::memcmp(caps_before, caps_after, sizeof caps_before) != 0)
+        drop_graphs(b);
     const long long C = b->tab_cap;
     std::vector<BInst> dev((size_t)C);
     std::memset(dev.data(), 0, sizeof(BInst) * (size_t)C);
@@ -278,7 +285,8 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
     if (d->nmat != b->nmat || d->dim != b->dim)
         return bfail(b, DIMGPU_E_INVALID_ARG, "instance nmat / dim differ from the batch's");
     if (d->time_update != DIMGPU_TIME_SPLIT) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs split steps only");
-    if (d->precision != DIMGPU_PRECISION_FP64) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs FP64 only");
+    if (d->precision != DIMGPU_PRECISION_FP64 && d->precision != DIMGPU_PRECISION_MIXED)
+        return bfail(b, DIMGPU_E_INVALID_ARG, "precision must be DIMGPU_PRECISION_FP64 or _MIXED");
     if (d->model != DIMGPU_MODEL_DIM) return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch runs the DIM step only");
     if (steps < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative step count");
     if (!(cfl > 0.0) || !(dt_max > 0.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "cfl and dt_max must be positive");
@@ -328,6 +336,7 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
     I.g.stride[1] = d->N[0];
     I.g.stride[2] = (long long)d->N[0] * d->N[1];
     I.steps_left = steps;
+    I.mixed = d->precision == DIMGPU_PRECISION_MIXED ? 1 : 0;
     I.cfl = cfl;
     I.dt_max = dt_max;
     const size_t bytes = sizeof(double) * (size_t)(2 * d->nmat + d->dim) * (size_t)ncell;

@@ -21,7 +21,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from .abi import Desc
+from .abi import PRECISION_MIXED, Desc
 from .batch import Batch
 
 # Device doubles per cell: two state copies plus the staged-sweep scratch
@@ -210,11 +210,12 @@ def sequential(requests: list[Request], clock=time.perf_counter, stream_handle=N
 
 
 def make_requests(n: int, rate: float, seed: int = 0, steps_range=(100, 2000), share_1d: float = 0.4,
-                  n1d_range=(256, 8192), side2d_range=(128, 2048)) -> list[Request]:
+                  n1d_range=(256, 8192), side2d_range=(128, 2048), share_mixed: float = 0.5) -> list[Request]:
     """Config 4 request stream: Poisson arrivals at `rate` per second; 40 %
     1D tubes (N log-uniform in n1d_range), 60 % 2D grids (sides log-uniform
     in side2d_range), steps uniform in steps_range, config-0/1 style seeded
-    initial conditions."""
+    initial conditions, a share_mixed fraction of them in the mixed-precision
+    form."""
     from . import workloads as W
     rng = np.random.default_rng(seed)
     t = 0.0
@@ -231,5 +232,7 @@ def make_requests(n: int, rate: float, seed: int = 0, steps_range=(100, 2000), s
                       for _ in range(2))
             d, U = W.riemann(seed=s, N=N, axis=int(rng.integers(0, 2))) if rng.uniform() < 0.5 \
                 else W.single_bubble_2d(N, seed=s)
+        if rng.uniform() < share_mixed:
+            d.precision = PRECISION_MIXED
         out.append(Request(k, d, U, steps, 0.6, 1e300, t))
     return out

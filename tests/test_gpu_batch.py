@@ -119,3 +119,52 @@ def test_batch_rejects_what_it_does_not_run():
         with pytest.raises(DimGpuError):
             b.add(d3, U3, 5, 0.5)
         assert len(b) == 0
+
+
+def test_mixed_precision_instances(port):
+    """Mixed-precision instances in a batch (alone and beside FP64 ones) end
+    bit for bit where a mixed-precision Session ends."""
+    cases = _cases_2d()[:6]
+    mixed = []
+    for k, (d, U, steps, cfl) in enumerate(cases):
+        dm = d.copy()
+        if k % 2 == 0:
+            dm.precision = abi.PRECISION_MIXED
+        mixed.append((dm, U, steps, cfl))
+    with Batch(2, 2) as b:
+        ids = [b.add(d, U, steps, cfl) for d, U, steps, cfl in mixed]
+        b.run(40)
+        for iid, (d, U, steps, cfl) in zip(ids, mixed):
+            out, dts = b.download(iid)
+            ref, rdts = _alone(d, U, steps, cfl)
+            assert ndiff(out, ref) == 0 and bitwise_equal(dts, rdts), (iid, d.precision)
+
+
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_graphs_dropped_when_the_scratch_regrows_in_place(precision):
+    """A leaves, a larger instance joins, runs from a captured graph, then a
+    third joins and the scratch regrows: the regrown scratch can come back at
+    the old address, so the captured graph (which bakes in the scratch
+    capacity that strides every record) must be dropped on the capacity
+    change too.  Every instance must still match its solve alone."""
+    from diffuse_vs_gfm_mms_b200 import serve
+    reqs = {r.rid: r for r in serve.make_requests(10, 200.0, seed=3, steps_range=(20, 60), n1d_range=(64, 512),
+                                                  side2d_range=(16, 64))}
+    for r in reqs.values():
+        r.desc.precision = precision
+    A, B, C = reqs[0], reqs[2], reqs[4]
+    with Batch(2, 2) as b:
+        ia = b.add(A.desc, A.U, A.steps, 0.6)
+        for _ in range(4):
+            b.run(8)
+        b.remove(ia)
+        ib = b.add(B.desc, B.U, B.steps, 0.6)
+        for _ in range(3):
+            b.run(8)
+        ic = b.add(C.desc, C.U, C.steps, 0.6)
+        b.run(8)
+        for iid, r in ((ib, B), (ic, C)):
+            done, _ = b.status(iid)
+            out, dts = b.download(iid)
+            ref, rdts = _alone(r.desc, r.U, done, 0.6)
+            assert ndiff(out, ref) == 0 and bitwise_equal(dts, rdts), r.rid
