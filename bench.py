@@ -182,6 +182,22 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(values, device="cuda"):
+    """Element-wise maximum of per-rank timings over the process group (the
+    slowest rank sets a replica run's time)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.tolist()]
+
+
+def replica_value(world: int, cells: int, steps: int, max_ms: float) -> float:
+    """Whole-job throughput of N replicas: every rank advanced `cells` cells
+    `steps` times; the job took as long as its slowest rank."""
+    return world * cells * steps / (max_ms * 1e-3)
+
+
 def dist_init():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -328,9 +344,7 @@ def run_ours(args):
 
     # ---- max over ranks
     if world > 1:
-        t = torch.tensor([total_ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms, e2e_ms = float(t[0]), float(t[1])
+        total_ms, e2e_ms = max_over_ranks([total_ms, e2e_ms], device="cuda")
 
     error_vs_fp64 = None
     if args.precision == "mixed":
@@ -354,8 +368,8 @@ def run_ours(args):
             dist.destroy_process_group()
         return
 
-    value = world * ncell * args.steps / (total_ms * 1e-3)
-    e2e_value = world * ncell * args.steps / (e2e_ms * 1e-3)
+    value = replica_value(world, ncell, args.steps, total_ms)
+    e2e_value = replica_value(world, ncell, args.steps, e2e_ms)
     sweep = prof["sweep"]
     avg_sweep_s = sweep["ms"] / max(sweep["launches"], 1) * 1e-3
     alg_bytes = 2 * V * 8 * ncell  # read + write of the state, per sweep launch
