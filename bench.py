@@ -376,7 +376,7 @@ def run_ours(args):
     achieved = alg_bytes / avg_sweep_s / 1e9
     peak, peak_src = measured_peaks()
     traffic, traffic_src = ncu_traffic(args.workload + ("-mixed" if args.precision == "mixed" else ""))
-    sched = "mixed staged sweep (staged_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
+    sched = "mixed staged sweep (mixed_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
         "staged sweep (staged_a..staged_e)"
     if args.workload in EULER_WORKLOADS:
         sched = "euler_sweep_kernel (fused tile)"

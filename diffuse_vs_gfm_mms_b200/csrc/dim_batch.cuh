@@ -45,7 +45,8 @@ __global__ void __launch_bounds__(256) batch_cfl(const BInst* __restrict__ tab, 
             State<NM, D> U;
             Prim<NM, D> P;
             load_cell<NM, D>(I.st[parity], I.g.ncell, c, U);
-            cons_to_prim<NM, D>(I.M, U, P);
+            if (I.mixed) cons_to_prim_mixed<NM, D>(I.M, U, P);
+            else cons_to_prim<NM, D>(I.M, U, P);
             best = cfl_candidate<NM, D>(I.M, U, P, I.g.dx, I.cfl, false);
         }
         best = warp_min(best);
@@ -123,7 +124,8 @@ __global__ void __launch_bounds__(256) batch_a(const BInst* __restrict__ tab, co
     State<NM, D> U;
     load_cell<NM, D>(in, I.g.ncell, it.cell, U);
     CellA<NM, D> A;
-    stage_a<NM, D>(I.M, U, A);
+    if (I.mixed) stage_a_mixed<NM, D>(I.M, U, A);
+    else stage_a<NM, D>(I.M, U, A);
     g_put<NM, D>(b.P, b.cap, q, A.P);
     g_put<NM, D>(b.Pe, b.cap, q, A.Pe);
 #pragma unroll

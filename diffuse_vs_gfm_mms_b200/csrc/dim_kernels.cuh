@@ -559,12 +559,33 @@ __global__ void __launch_bounds__(256) staged_e(const double* __restrict__ in, d
 
 // ---- the mixed-precision staged sweep (precision MIXED) ---------------------------
 //
-// Stage A and stage E are staged_a / staged_e (FP64 cell recovery, FP64 cell
-// update).  mixed_b is stage B with FP32-limited slopes and no face-state
+// Stage A is mixed_a (staged_a with the closed-form FP64 recovery), stage E
+// is staged_e (FP64 cell update).  mixed_b is stage B with FP32-limited slopes and no face-state
 // round trip; mixed_cd builds the two face states of face i|i+1 from the
 // half-step primitives of cells i-1..i+2 and runs the FP32-increment HLLC,
 // so the face states never reach HBM.  Scratch: P, ck, Pe, Ph and the face
 // records, at the staged positions.
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+                                               StagedBufs<NM, D> b, FusedCfl fc)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double best = HUGE_VAL;
+    if (t < (long long)ls.nl * ls.n) {
+        const StagedItem<DIR> it(g, ls, t);
+        State<NM, D> U;
+        load_cell<NM, D>(in, g.ncell, it.cell, U);
+        CellA<NM, D> A;
+        stage_a_mixed<NM, D>(M, U, A);
+        g_put<NM, D>(b.P, b.cap, t, A.P);
+        g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
+#pragma unroll
+        for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
+        if (fc.on) best = cfl_candidate<NM, D>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+    }
+    if (fc.on) fused_cfl_reduce(best, fc);
+}
+
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) mixed_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
                                                StagedBufs<NM, D> b, const double* __restrict__ dtp)
@@ -656,7 +677,7 @@ __device__ __forceinline__ double warp_min(double v)
 
 template<int NM, int D>
 __global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st, Grid g, Mats M, double cfl,
-                                                  int unsplit, double* __restrict__ blockmin)
+                                                  int unsplit, int mixed, double* __restrict__ blockmin)
 {
     __shared__ double red[32];
     double best = HUGE_VAL;
@@ -665,7 +686,8 @@ __global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st,
         State<NM, D> U;
         Prim<NM, D> P;
         load_cell<NM, D>(st, g.ncell, i, U);
-        cons_to_prim<NM, D>(M, U, P);
+        if (mixed) cons_to_prim_mixed<NM, D>(M, U, P);  // the mixed step's own recovery
+        else cons_to_prim<NM, D>(M, U, P);
         best = dmin(best, cfl_candidate<NM, D>(M, U, P, g.dx, cfl, unsplit != 0));
     }
     best = warp_min(best);
@@ -1035,7 +1057,7 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
         const unsigned blocks = (unsigned)((items + 255) / 256);
         FusedCfl fc{0, 0, 0.0, nullptr};
         if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
-        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
+        mixed_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
         count_launches(1);
         if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
         mixed_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
@@ -1068,13 +1090,13 @@ cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const doub
 
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
-                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s)
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed)
 {
     long long nb = (g.ncell + 255) / 256;
     if (nb > max_blocks) nb = max_blocks;
     if (nb < 1) nb = 1;
     *nblocks = (int)nb;
-    cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, blockmin);
+    cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, mixed ? 1 : 0, blockmin);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -1245,7 +1267,7 @@ cudaError_t launch_boundary_flux(const Grid& g, const Mats& M, const double* sta
                                                    const double*, int*, double*, long long, const FusedStep&, \
                                                    cudaStream_t);                                            \
     template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
-                                           int, int*, cudaStream_t);                                         \
+                                           int, int*, cudaStream_t, bool);                                   \
     template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \
     template cudaError_t launch_accumulate<NM, D>(const Grid&, const Mats&, double*, const double*,          \
                                                   const double*, cudaStream_t);                              \

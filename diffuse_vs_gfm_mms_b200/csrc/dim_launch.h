@@ -74,9 +74,10 @@ cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const doub
                                cudaStream_t s);
 
 // Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
+// `mixed`: recover the cells as the mixed-precision step does.
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
-                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s);
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed = false);
 
 // dt = min(dt_max, min(blockmin)), written to dt[0] and hist[0] (hist may be null).
 cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_max, double* dt,

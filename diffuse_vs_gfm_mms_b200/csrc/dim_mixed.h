@@ -12,9 +12,10 @@
 //    star-state ratios (chi - 1, s* - u_K, s_K rho_K (s* - u_K)) are FP32,
 //    and the flux is FP64 state times FP64 coefficients built from them;
 //  * FP64: the cell recoveries (cons_to_prim of U and of the half-step
-//    state, where (gamma-1)(E - kinetic) - gamma p_inf cancels), every
-//    sound speed and wave-speed estimate, the physical fluxes, the Hancock
-//    and cell updates, the alpha update and the CFL dt.
+//    state, where (gamma-1)(E - kinetic) - gamma p_inf cancels; in closed
+//    form, pressure_closed_form below), every sound speed and wave-speed
+//    estimate, the physical fluxes, the Hancock and cell updates, the alpha
+//    update and the CFL dt.
 // A face state is built from its reconstructed primitive without the FP64
 // step's repair / re-recovery round trip (prim_to_cons -> repair_state ->
 // cons_to_prim), and HLLC takes the reconstructed primitive itself; the
@@ -75,6 +76,70 @@ DHD void reconstruct_mixed(const Prim<NM, D>& PL, const Prim<NM, D>& PC, const P
     Rf.p = PC.p + h;
     enforce_positive_primitive<NM, D>(Lf);
     enforce_positive_primitive<NM, D>(Rf);
+}
+
+// The mixed form's pressure recovery: for ideal and stiffened gases the
+// residual the reference bisects (pressure_from_internal_energy,
+// src/dim/eos.hpp:77-143) is affine in p above its 1e-10 clamp,
+// f(p) = A p + B - rho e, so its root is (rho e - B) / A in FP64, one
+// subtraction (where the gamma p_inf terms cancel) and one division.  The
+// bisection stops anywhere within 1e-10 * max(1, rho e) / A of that root; the
+// mixed step takes the root itself.  Where the root is not a plain positive
+// number above 1e-8 (the reference then falls back or clamps), the reference
+// bisection runs instead.
+template<int NM>
+DHD double pressure_closed_form(const Mats& M, double rho_total, double e, const double* alpha, const double* rho)
+{
+    const double rt = clamp_min(rho_total);
+    const double target = finite_or(rt * finite_or(e));
+    double A = 0.0, B = 0.0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        const double alpha_k = dmax(finite_or(alpha[k]), 0.0);
+        const double rho_k = clamp_min(rho[k]);
+        const double w = (alpha_k * rho_k) / safe_denom(M.gm1[k] * rho_k);
+        A += w;
+        if (M.stiff[k]) B += w * M.gpinf[k];
+    }
+    const double p = (target - B) / A;
+    if (fin(A) && fin(B) && A > 1e-200 && fin(p) && p >= 1e-8 && p < 1e290 / A) return p;
+    return pressure_from_internal_energy<NM>(M, rho_total, e, alpha, rho);
+}
+
+// cons_to_prim (primitives.hpp:111-162) with the closed-form recovery.
+template<int NM, int D>
+DNI void cons_to_prim_mixed(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+{
+    full_alpha<NM, D>(U, P.alpha);
+    sanitise_alpha<NM>(P.alpha, 1e-12);
+    double rho_total = 0.0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) rho_total += finite_or(U.m[k]);
+    rho_total = dmax(rho_total, 1e-12);
+    double velocity_squared = 0.0;
+#pragma unroll
+    for (int d = 0; d < D; ++d) {
+        P.vel[d] = safe_div(U.mom[d], rho_total);
+        velocity_squared += P.vel[d] * P.vel[d];
+    }
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        const double alpha_k = dmax(P.alpha[k], 1e-12);
+        P.rho[k] = dmax(safe_div(finite_or(U.m[k]), alpha_k), 1e-12);
+    }
+    const double kinetic = 0.5 * rho_total * velocity_squared;
+    const double internal_energy = safe_div(finite_or(U.E, kinetic) - kinetic, rho_total);
+    P.p = dmax(pressure_closed_form<NM>(M, rho_total, internal_energy, P.alpha, P.rho), 1e-12);
+}
+
+// Stage A of the mixed step (stage_a with the closed-form recovery).
+template<int NM, int D>
+DHD void stage_a_mixed(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
+{
+    cons_to_prim_mixed<NM, D>(M, U, A.P);
+    A.Pe = A.P;
+    enforce_positive_primitive<NM, D>(A.Pe);
+    rhs_sound_speeds<NM, D>(M, A.P, A.ck);
 }
 
 // HLLC with the star state in FP32 increment form.  Same wave-speed
@@ -214,7 +279,7 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) Uh.a[k] = alpha_new[k];
     repair_state<NM, D>(M, Uh);
-    cons_to_prim<NM, D>(M, Uh, Ph);
+    cons_to_prim_mixed<NM, D>(M, Uh, Ph);
     enforce_positive_primitive<NM, D>(Ph);
 }
 

@@ -273,7 +273,7 @@ cudaError_t run_cfl(dimgpu_session* s, double cfl, double dt_max, double* hist)
         else {
             DISPATCH_ND(s->desc.nmat, s->desc.dim,
                         e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks,
-                                              &nb, s->stream));
+                                              &nb, s->stream, s->desc.precision == DIMGPU_PRECISION_MIXED));
         }
     }
     if (e != cudaSuccess) return e;

@@ -118,7 +118,7 @@ int solve_line_mixed(const Mats& M, int n, const State<NM, D>* U, State<NM, D>* 
     std::vector<Prim<NM, D>> Ph(n);
     std::vector<FaceD<NM, D>> F(n);
     auto is_end = [&](int i) { return i == 0 || i == n - 1 || n < 3; };
-    for (int i = 0; i < n; ++i) stage_a<NM, D>(M, U[i], A[i]);
+    for (int i = 0; i < n; ++i) stage_a_mixed<NM, D>(M, U[i], A[i]);
     for (int i = 0; i < n; ++i) {
         const Prim<NM, D>& lo = A[i > 0 ? i - 1 : i].Pe;
         const Prim<NM, D>& hi = A[i < n - 1 ? i + 1 : i].Pe;

@@ -1,6 +1,6 @@
 """The mixed-precision form (FP32 slope limiting and HLLC star increments;
-FP64 state, physical fluxes, updates, mixture pressure / sound-speed
-recovery and dt): its error against the FP64 oracle, per conserved
+FP64 state, physical fluxes, updates, closed-form mixture pressure /
+sound-speed recovery and dt): its error against the FP64 oracle, per conserved
 variable, after 100 steps.
 
 Two kinds of case.  On a well-conditioned problem (ideal-gas mixtures) the
@@ -70,7 +70,7 @@ def _report(name, out, ref, dts, rdts, d=None):
 
 # Transverse momentum of the shock-bubble run is ~1 % of the axial one, so
 # its relative L1 magnifies absolute errors ~100x.  There the mixed form
-# measures 1.4e-6: not FP32 rounding, but the face states built without the
+# measures ~1.6e-6: not FP32 rounding, but the face states built without the
 # FP64 step's repair / re-recovery round trip, whose bisection leaves each
 # face pressure within 1e-10 * rho e of the reconstructed one (the FP64 step
 # with only that round trip removed measures 1.9e-6 on the same variable).
