@@ -1,6 +1,6 @@
 """Parity of the CUDA DIM step with the CPU oracle and the reference's golden
 vectors, through the C-ABI (libdimgpu.so).  The bar is bit-for-bit equality;
-the north-star tolerance (1e-10 relative L1 per conserved variable after 100
+the parity target (1e-10 relative L1 per conserved variable after 100
 steps) is asserted as well so a failure says by how much it missed."""
 from __future__ import annotations
 
