@@ -368,9 +368,22 @@ def run_ours(args):
         scale = den2[mom].max()
         den2[mom] = np.where(den2[mom] < 1e-6 * scale, scale, den2[mom])
         l1s = np.abs(mixed_out - ref).sum(axis=1) / np.where(den2 > 0, den2, 1.0)
+        # the FP64 step's own conditioning on this input: its response to a
+        # seeded 1e-15 relative perturbation of the initial state, after the
+        # same steps (a stiffened gas far below gamma * p_inf amplifies it)
+        rng = np.random.default_rng(7)
+        Up = U.copy()
+        for c in range(Up.shape[0]):
+            Up[c] *= 1.0 + 1e-15 * rng.standard_normal(Up.shape[1:])
+        with Session(d64, Up) as sp:
+            sp.steps(nsteps, cfl, 1e300)
+            pert = sp.download()
+        del Up
+        sens = np.abs(pert - ref).sum(axis=1) / np.where(den > 0, den, 1.0)
         error_vs_fp64 = {"steps": nsteps, "rel_l1_per_variable": [float(x) for x in l1],
                          "rel_linf_per_variable": [float(x) for x in linf], "max_rel_l1": float(l1.max()),
-                         "max_rel_l1_zero_momentum_scored": float(l1s.max())}
+                         "max_rel_l1_zero_momentum_scored": float(l1s.max()),
+                         "fp64_rel_l1_response_to_1e-15_input_perturbation": [float(x) for x in sens]}
     s.close()
     if rank != 0:
         if world > 1:
