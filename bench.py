@@ -129,18 +129,65 @@ def ncu_traffic(workload: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clocks and throttle reasons sampled during the timed region.
+
+    A thread reads NVML (the library nvidia-smi reports from) every 2 ms, so
+    that even a timed region of a few milliseconds holds several samples;
+    without NVML, nvidia-smi is polled every 200 ms and the region may fall
+    between two of its samples."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.thread = None
         self.path = os.path.join("/tmp", f"dimgpu_clocks_{os.getpid()}.csv")
+        self.sm, self.smax, self.reasons = [], None, set()
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.index)
+            bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
+
+    def _poll(self, nv, h):
+        get_reasons = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+            nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        masks = [(name, getattr(nv, attr, bit)) for name, attr, bit in self.REASONS]
+        while not self.stop.is_set():
+            try:
+                self.sm.append(float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)))
+                bits = get_reasons(h)
+                for name, m in masks:
+                    if bits & m:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self.stop.wait(0.002)
 
     def __enter__(self):
+        try:
+            import threading
+            nv, h = self._nvml_handle()
+            self.smax = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.stop = threading.Event()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            return self
+        except Exception:
+            self.thread = None
         try:
             self.f = open(self.path, "w")
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
@@ -151,6 +198,9 @@ class ClockSampler:
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -160,10 +210,14 @@ class ClockSampler:
             self.f.close()
 
     def summary(self):
+        if self.thread:
+            sm = self.sm
+            return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": self.smax,
+                    "samples": len(sm), "source": "nvml every 2 ms", "reasons": sorted(self.reasons)}
         if not self.proc or not os.path.exists(self.path):
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
         sm, smax, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        names = [r[0] for r in self.REASONS]
         with open(self.path) as f:
             for line in f:
                 parts = [p.strip() for p in line.split(",")]
@@ -179,7 +233,7 @@ class ClockSampler:
                         reasons.add(nm)
         os.unlink(self.path)
         return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax,
-                "samples": len(sm), "reasons": sorted(reasons)}
+                "samples": len(sm), "source": "nvidia-smi every 200 ms", "reasons": sorted(reasons)}
 
 
 def max_over_ranks(values, device="cuda"):

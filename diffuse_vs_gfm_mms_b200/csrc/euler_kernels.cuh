@@ -96,8 +96,12 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // buffers of V = D + 2 doubles per slot: S0 holds P (A -> B), then RS
 // (C -> D); S1 holds Ph (B -> C), then the face flux F (D -> E); S2 holds LS
 // (C -> D).
+//
+// Launch bound: 4 blocks of 256 threads per SM (64 registers a thread).  The
+// sweep is latency-bound on dependent FP64 chains; the extra warps hide more
+// of that latency than the few spilled registers (L1-resident) cost.
 template<int D, int DIR>
-__global__ void __launch_bounds__(256, 3) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
+__global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                              Grid g, Mats M, int T, int W, int ntile, int ngx,
                                                              const double* __restrict__ dtp, int* __restrict__ err,
                                                              int ends_copy)
