@@ -589,7 +589,8 @@ __global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, Gr
 // mixed_b and mixed_cd run 3 blocks of 256 threads per SM (at most 85
 // registers a thread, a few spilled to L1) rather than the 2 that ~100
 // registers allow: the FP64 chains are latency-bound, and the extra warps
-// cut the mixed step's time by 2.5 % (c1) and 1.2 % (c2 at 256^3) on a B200.
+// cut the mixed step's time on a B200 by 2.5 % (2D shock-bubble 1024x512)
+// and 1.2 % (3D bubble cloud 256^3).
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)
