@@ -865,7 +865,7 @@ __global__ void bc_serial_kernel(double* st, Grid g, Mats M)
     }
 }
 
-// ---- unsplit accumulation (src/dim/solver/advance_step.hpp:198-222) -------------
+// ---- unsplit accumulation (src/dim/solver/advance_step.hpp:77-101) -------------
 template<int NM, int D>
 __global__ void __launch_bounds__(256) accumulate_kernel(double* __restrict__ acc, const double* __restrict__ dir_state,
                                                          const double* __restrict__ base, Grid g, Mats M)

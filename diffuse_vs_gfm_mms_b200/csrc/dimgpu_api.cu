@@ -1,6 +1,6 @@
 // dimgpu_api.cu — the C-ABI (include/dimgpu.h): sessions owning the
 // device-resident SoA state, the step orchestration of dim::advance_one_step
-// (src/dim/solver/advance_step.hpp:150-270) and the stateless drop-in call.
+// (src/dim/solver/advance_step.hpp:29-149) and the stateless drop-in call.
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -10,6 +10,7 @@
 
 #include "dim_launch.h"
 #include "dimgpu.h"
+#include "dimgpu_validate.h"
 
 using namespace dimgpu;
 
@@ -202,42 +203,9 @@ int cuda_fail(dimgpu_session* s, cudaError_t e, const char* what)
 
 int validate_desc(const dimgpu_desc* d, std::string* where)
 {
-    if (!d) return fail(where, DIMGPU_E_INVALID_ARG, "null descriptor");
-    if (d->dim < 1 || d->dim > 3) return fail(where, DIMGPU_E_INVALID_ARG, "dim must be 1, 2 or 3");
-    if (d->nmat < 1 || d->nmat > DIMGPU_MAX_MATERIALS)
-        return fail(where, DIMGPU_E_INVALID_ARG, "dim::EOSParams: nmat must be 1..4");
-    for (int a = 0; a < 3; ++a) {
-        const int n = d->N[a];
-        if (a < d->dim && n < 1) return fail(where, DIMGPU_E_INVALID_ARG, "dim::total_cells: grid size must be positive");
-        if (a >= d->dim && n != 1) return fail(where, DIMGPU_E_INVALID_ARG, "unused axes must have N = 1");
-        if (a < d->dim && !(d->dx[a] > 0.0))
-            return fail(where, DIMGPU_E_INVALID_ARG, "dim::compute_dt_cfl: grid spacing must be positive");
-    }
-    for (int k = 0; k < d->nmat; ++k) {
-        const int kind = d->mat[k].kind;
-        if (kind != DIMGPU_EOS_IDEAL_GAS && kind != DIMGPU_EOS_STIFFENED_GAS)
-            return fail(where, DIMGPU_E_UNSUPPORTED_EOS,
-                        "material " + std::to_string(k) + ": only ideal_gas and stiffened_gas run on the GPU");
-        if (!(d->mat[k].gamma > 1.0)) return fail(where, DIMGPU_E_INVALID_ARG, "dim::EOSParams: gamma must be > 1");
-    }
-    if (d->lambda_model < 0 || d->lambda_model > 2)
-        return fail(where, DIMGPU_E_INVALID_ARG, "dim::alpha_rhs_coefficients: unknown lambda model");
-    if (d->precision != DIMGPU_PRECISION_FP64 && d->precision != DIMGPU_PRECISION_MIXED)
-        return fail(where, DIMGPU_E_INVALID_ARG, "precision must be DIMGPU_PRECISION_FP64 or _MIXED");
-    if (d->time_update != DIMGPU_TIME_SPLIT && d->time_update != DIMGPU_TIME_UNSPLIT)
-        return fail(where, DIMGPU_E_INVALID_ARG, "time_update must be split or unsplit");
-    if (d->model != DIMGPU_MODEL_DIM && d->model != DIMGPU_MODEL_EULER)
-        return fail(where, DIMGPU_E_INVALID_ARG, "model must be DIMGPU_MODEL_DIM or DIMGPU_MODEL_EULER");
-    if (d->model == DIMGPU_MODEL_EULER) {
-        if (d->nmat != 1)
-            return fail(where, DIMGPU_E_INVALID_ARG, "the Euler step runs exactly one material (nmat = 1)");
-        if (d->precision != DIMGPU_PRECISION_FP64)
-            return fail(where, DIMGPU_E_UNSUPPORTED, "the Euler step runs in FP64 only");
-        for (int a = 0; a < d->dim; ++a)
-            if (d->N[a] < 3)
-                return fail(where, DIMGPU_E_INVALID_ARG, "reconstruct_line_interfaces: need at least 3 cells");
-    }
-    return DIMGPU_OK;
+    std::string msg;
+    const int rc = check_desc(d, &msg);
+    return rc ? fail(where, rc, msg) : DIMGPU_OK;
 }
 
 int check_err(dimgpu_session* s)

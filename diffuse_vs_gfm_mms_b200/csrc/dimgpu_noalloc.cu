@@ -25,6 +25,7 @@
 
 #include "dim_launch.h"
 #include "dimgpu.h"
+#include "dimgpu_validate.h"
 
 using namespace dimgpu;
 
@@ -74,33 +75,22 @@ extern "C" int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const doub
                                              double dt_max, double* dt_out, void* cuda_stream)
 {
     if (!desc || !d_state || !dt_out) return noalloc_fail(DIMGPU_E_INVALID_ARG, "null argument");
-    if (desc->dim < 1 || desc->dim > 3) return noalloc_fail(DIMGPU_E_INVALID_ARG, "dim must be 1, 2 or 3");
-    if (desc->nmat < 1 || desc->nmat > DIMGPU_MAX_MATERIALS)
-        return noalloc_fail(DIMGPU_E_INVALID_ARG, "nmat must be 1..4");
+    {
+        std::string msg;
+        const int rc = check_desc(desc, &msg);
+        if (rc) return noalloc_fail(rc, msg);
+    }
+    // The cell count is checked against the limit axis by axis, so the
+    // product never grows past kMaxCells * INT_MAX (no signed overflow).
     long long ncell = 1;
     for (int a = 0; a < 3; ++a) {
-        const int n = desc->N[a];
-        if (a < desc->dim && n < 1) return noalloc_fail(DIMGPU_E_INVALID_ARG, "grid size must be positive");
-        if (a >= desc->dim && n != 1) return noalloc_fail(DIMGPU_E_INVALID_ARG, "unused axes must have N = 1");
-        if (a < desc->dim && !(desc->dx[a] > 0.0))
-            return noalloc_fail(DIMGPU_E_INVALID_ARG, "grid spacing must be positive");
-        ncell *= n;
+        ncell *= desc->N[a];
+        if (ncell > kMaxCells)
+            return noalloc_fail(DIMGPU_E_INVALID_ARG,
+                                "grid " + std::to_string(desc->N[0]) + " x " + std::to_string(desc->N[1]) + " x " +
+                                    std::to_string(desc->N[2]) + " exceeds the allocation-free limit of " +
+                                    std::to_string(kMaxCells) + " cells");
     }
-    if (ncell > kMaxCells)
-        return noalloc_fail(DIMGPU_E_INVALID_ARG,
-                            "grid of " + std::to_string(ncell) + " cells exceeds the allocation-free limit of " +
-                                std::to_string(kMaxCells) + " cells");
-    for (int k = 0; k < desc->nmat; ++k) {
-        if (desc->mat[k].kind != DIMGPU_EOS_IDEAL_GAS && desc->mat[k].kind != DIMGPU_EOS_STIFFENED_GAS)
-            return noalloc_fail(DIMGPU_E_UNSUPPORTED_EOS, "only ideal_gas and stiffened_gas run on the GPU");
-        if (!(desc->mat[k].gamma > 1.0)) return noalloc_fail(DIMGPU_E_INVALID_ARG, "gamma must be > 1");
-    }
-    if (desc->lambda_model < 0 || desc->lambda_model > 2)
-        return noalloc_fail(DIMGPU_E_INVALID_ARG, "unknown lambda model");
-    if (desc->model != DIMGPU_MODEL_DIM && desc->model != DIMGPU_MODEL_EULER)
-        return noalloc_fail(DIMGPU_E_INVALID_ARG, "unknown model");
-    if (desc->model == DIMGPU_MODEL_EULER && desc->nmat != 1)
-        return noalloc_fail(DIMGPU_E_INVALID_ARG, "the Euler step runs exactly one material");
     if (!(cfl > 0.0)) return noalloc_fail(DIMGPU_E_INVALID_ARG, "cfl must be positive");
     if (!(dt_max > 0.0)) return noalloc_fail(DIMGPU_E_INVALID_ARG, "dt_max must be positive");
 

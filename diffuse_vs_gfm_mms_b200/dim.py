@@ -1,6 +1,6 @@
 """Python face of the DIM step, mirroring the reference's call surface.
 
-The reference (src/dim/solver/advance_step.hpp:150-270) exposes
+The reference (src/dim/solver/advance_step.hpp:29-149) exposes
 ``dim::advance_one_step<DIM>(U, N, dx, params, cfg, cfl, dt_max) ->
 StepResult{U_new, dt, phase_timings}`` with ``compute_dt_cfl``,
 ``sweep_direction_dispatch`` and ``apply_boundary_conditions`` beneath it.
@@ -28,7 +28,7 @@ __all__ = ["Session", "StepResult", "advance_one_step", "DimGpuError"]
 
 @dataclass
 class StepResult:
-    """dim::StepResult (src/dim/solver/advance_step.hpp:140-146); times in seconds."""
+    """dim::StepResult (src/dim/solver/advance_step.hpp:20-25); times in seconds."""
     U_new: np.ndarray
     dt: float
     phase_timings: dict = field(default_factory=dict)

@@ -98,7 +98,7 @@ enum {
 
 /* Which step a session runs. */
 enum {
-    DIMGPU_MODEL_DIM = 0,   /* dim::advance_one_step (src/dim/solver/advance_step.hpp:150) */
+    DIMGPU_MODEL_DIM = 0,   /* dim::advance_one_step (src/dim/solver/advance_step.hpp:29) */
     DIMGPU_MODEL_EULER = 1  /* the single-material Euler step: advance_one_step<DIM, EOS>
                              * (src/sim/solver/advance_step.hpp:489) with one material
                              * and no level set; nmat = 1, V = 2 + DIM components
@@ -115,7 +115,7 @@ typedef struct dimgpu_material {
 } dimgpu_material;
 
 /* Everything the reference's step reads from N, dx, dim::EOSParams and
- * Config<DIM> (src/dim/solver/advance_step.hpp:150-158). */
+ * Config<DIM> (src/dim/solver/advance_step.hpp:28-37). */
 typedef struct dimgpu_desc {
     int dim;                        /* 1, 2 or 3                                  */
     int N[3];                       /* cells per axis; unused axes must be 1      */
@@ -158,16 +158,16 @@ const char* dimgpu_last_error(const dimgpu_session* s);
 
 /* Copy `count` doubles (must be V * ncell) from a host SoA buffer into the
  * session.  Replaces the caller's std::vector<dim::State<DIM>> argument of
- * dim::advance_one_step (src/dim/solver/advance_step.hpp:150-151). */
+ * dim::advance_one_step (src/dim/solver/advance_step.hpp:29-31). */
 int dimgpu_upload(dimgpu_session* s, const double* soa, size_t count);
 
 /* Copy the session state into a host SoA buffer of `count` doubles.
- * Replaces StepResult::U_new (src/dim/solver/advance_step.hpp:141-146). */
+ * Replaces StepResult::U_new (src/dim/solver/advance_step.hpp:20-25, 147). */
 int dimgpu_download(dimgpu_session* s, double* soa, size_t count);
 
 /* One full time step on the resident state: CFL dt, then the split x, y, z
  * sweeps, each followed by the boundary fill.  Replaces
- * dim::advance_one_step (src/dim/solver/advance_step.hpp:150-270).
+ * dim::advance_one_step (src/dim/solver/advance_step.hpp:29-149).
  * dt_out receives the step's dt; times may be NULL. */
 int dimgpu_step(dimgpu_session* s, double cfl, double dt_max, double* dt_out,
                 dimgpu_phase_times* times);
@@ -256,7 +256,11 @@ long long dimgpu_kernel_launches(void);
  * d_state: device pointer to the SoA state (layout above); the result is
  * written to the host double *dt_out; work runs on `cuda_stream` (a
  * cudaStream_t cast to void*, NULL for the default stream) and the call
- * returns once dt is on the host.  Same value as dimgpu_compute_dt_cfl.
+ * returns once dt is on the host.  Same value as dimgpu_compute_dt_cfl, and
+ * the same descriptor checks.  One difference: for the Euler model a
+ * non-finite density returns DIMGPU_E_NONFINITE here (the reference's
+ * compute_dt_cfl_materials throws there), where dimgpu_compute_dt_cfl
+ * returns the dt and leaves the decision to the step that follows.
  *
  * Limits: at most 4 194 304 cells (larger grids return DIMGPU_E_INVALID_ARG
  * before any device work).  The scratch is one 128 KB array per GPU, static
@@ -267,7 +271,7 @@ int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const double* d_state
                                   double dt_max, double* dt_out, void* cuda_stream);
 
 /* Stateless drop-in for one call of dim::advance_one_step
- * (src/dim/solver/advance_step.hpp:150-270): host SoA in, host SoA out.
+ * (src/dim/solver/advance_step.hpp:29-149): host SoA in, host SoA out.
  * Uses a cached session per descriptor shape; the copies are part of the call. */
 int dimgpu_advance_one_step(const dimgpu_desc* desc, const double* soa_in, double* soa_out,
                             double cfl, double dt_max, double* dt_out,

@@ -6,7 +6,7 @@
 //   dimgpu::advance_one_step<DIM>(U, N, dx, params, cfg, cfl, dt_max)
 //
 // with exactly the signature and return type of dim::advance_one_step
-// (src/dim/solver/advance_step.hpp:150-158), so a caller such as run_dim_case
+// (src/dim/solver/advance_step.hpp:28-37), so a caller such as run_dim_case
 // (src/app/solver/run_dim.hpp:94) switches by changing the namespace, and
 // dimgpu::ResidentDim<DIM>, which keeps the state on the GPU across steps and
 // converts the reference's AoS std::vector<dim::State<DIM>> to and from the

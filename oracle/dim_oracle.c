@@ -1154,7 +1154,7 @@ int oracle_apply_boundary_conditions(const dimgpu_desc* d, double* soa)
     return 0;
 }
 
-/* src/dim/solver/advance_step.hpp:150-270 (split and unsplit). */
+/* src/dim/solver/advance_step.hpp:29-149 (split and unsplit). */
 int oracle_advance(const dimgpu_desc* d, const double* soa_in, double* soa_out, double cfl,
                    double dt_max, int nsteps, double* dt_out)
 {

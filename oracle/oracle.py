@@ -25,9 +25,12 @@ PORT_SO = os.path.join(HERE, "_build", "libdimoracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libdimref.so")
 
 
-def build(quiet: bool = True) -> None:
-    """Compile the C restatement (and the reference where its sources exist)."""
-    out = subprocess.run(["make", "-C", HERE], capture_output=True, text=True)
+def build(quiet: bool = True, ref_src: str | None = None) -> None:
+    """Compile the C restatement, and the reference from its sources when
+    `ref_src` (or $DIMGPU_REFERENCE_SRC) names a checkout of it."""
+    ref_src = ref_src or os.environ.get("DIMGPU_REFERENCE_SRC", "")
+    cmd = ["make", "-C", HERE] + ([f"REF={ref_src}"] if ref_src else [])
+    out = subprocess.run(cmd, capture_output=True, text=True)
     if out.returncode != 0:
         raise RuntimeError("oracle build failed:\n" + out.stdout + out.stderr)
     if not quiet:
