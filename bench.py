@@ -76,34 +76,26 @@ def make_workload(name: str, scale: int = 1):
 
 
 def reference_sample(name: str):
-    """The bounded CPU sample of a workload: same spacing and physics, fewer lines."""
+    """What the CPU reference runs for a workload: the whole grid wherever
+    the reference can hold and step it in seconds (c0, c1, e2); a block of
+    the grid at the same spacing where it cannot (c2 at 512^3 needs ~95 GB of
+    host memory, e3 ~7 s per step)."""
     from diffuse_vs_gfm_mms_b200 import workloads as W
-    if name == "c1":
-        d, U = W.shock_bubble_2d(N=(1024, 512))
-        # a strip of 64 rows x 1024 columns around the bubble's centre line
-        V = d.nvar
-        U3 = U.reshape(V, 512, 1024)[:, 224:288, :]
-        d2 = d.copy()
-        d2.N[1] = 64
-        return d2, np.ascontiguousarray(U3.reshape(V, -1)), "1024x64 strip of the 1024x512 grid (rows 224-287)"
+    if name in ("c0", "c1", "e2"):
+        d, U = make_workload(name)
+        return d, U, "the whole grid"
     if name == "c2":
         d, U = W.bubble_cloud_3d(N=(64, 64, 64), nbubbles=64)
         d.dx[0] = d.dx[1] = d.dx[2] = 1.0 / 512
         return d, U, "64^3 block of the 512^3 case (same spacing, 64 bubbles)"
-    if name in ("e2", "e3"):
+    if name == "e3":
         d, U = make_workload(name)
         V = d.nvar
-        if name == "e2":
-            U3 = U.reshape(V, 2048, 2048)[:, 992:1056, :]
-            d2 = d.copy()
-            d2.N[1] = 64
-            return d2, np.ascontiguousarray(U3.reshape(V, -1)), "2048x64 strip through the blast centre"
         U4 = U.reshape(V, 256, 256, 256)[:, 112:144, :, :]
         d2 = d.copy()
         d2.N[2] = 32
         return d2, np.ascontiguousarray(U4.reshape(V, -1)), "256x256x32 slab through the blast centre"
-    d, U = W.riemann(seed=0, N=(1000,))
-    return d, U, "the whole 1000-cell tube"
+    raise SystemExit(f"no CPU reference for workload {name}")
 
 
 def measured_peaks():
@@ -115,17 +107,43 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
-def ncu_traffic(workload: str):
-    """dram bytes (read + write) per sweep (all kernels of one sweep) from the
-    committed ncu summaries: a line `traffic_bytes_per_launch <workload>
-    <bytes>` (workload `c1`, or `c1-mixed` for the mixed-precision form)."""
+def _profile_figure(key: str, workload: str):
+    """A per-launch figure from the committed ncu summaries under profiles/:
+    a line `<key> <workload> <value>` (workload `c1`, or `c1-mixed` for the
+    mixed-precision form)."""
     for path in sorted(glob.glob(os.path.join(ROOT, "profiles", "*.md"))):
         with open(path) as f:
             for line in f:
-                m = re.match(r"\s*traffic_bytes_per_launch\s+(\S+)\s+([0-9.eE+]+)", line)
+                m = re.match(r"\s*" + re.escape(key) + r"\s+(\S+)\s+([0-9.eE+]+)", line)
                 if m and m.group(1) == workload:
                     return float(m.group(2)), os.path.relpath(path, ROOT)
     return None, None
+
+
+def ncu_traffic(workload: str):
+    """DRAM bytes (read + write) per sweep (all kernels of one sweep)."""
+    return _profile_figure("traffic_bytes_per_launch", workload)
+
+
+def ncu_fp64_flops_per_cell(workload: str):
+    """FP64 operations per cell and sweep (DADD + DMUL + 2 DFMA thread
+    instructions of one sweep's kernels, divided by the cells swept)."""
+    return _profile_figure("fp64_flops_per_cell_sweep", workload)
+
+
+def fp64_peak():
+    """Measured FP64 throughput of this GPU: a DFMA loop with eight
+    independent chains per thread on every SM (libdimprobe.so), timed with
+    CUDA events; the best of five launches, in FLOP/s (2 per DFMA)."""
+    import ctypes as C
+    path = os.path.join(ROOT, "diffuse_vs_gfm_mms_b200", "libdimprobe.so")
+    if not os.path.exists(path):
+        return None
+    lib = C.CDLL(path)
+    inst, flops = C.c_double(), C.c_double()
+    if lib.dimprobe_fp64_peak(5, C.byref(inst), C.byref(flops)) != 0:
+        return None
+    return flops.value
 
 
 class ClockSampler:
@@ -259,9 +277,13 @@ def dist_init():
     return world, rank, local
 
 
-def cpu_reference_rate(workload: str, steps: int, warmup: int):
-    """The reference's OpenMP code (oracle/_ref) on the host cores, on the
-    bounded sample of the workload; falls back to the C restatement."""
+def cpu_reference_rate(workload: str, steps: int, warmup: int = 1, repeats: int = 3):
+    """The reference's OpenMP code (oracle/_ref) on all host cores, run the
+    way its performance suite runs it (scripts/run_report2_local.sh:13-14,
+    tools/quant/runner.hpp:326-333): the runner's OpenMP settings, `warmup`
+    untimed steps, then `repeats` timed repeats of `steps` steps from the
+    same warmed state, and the median rate.  Falls back to the C
+    restatement where the reference was not built."""
     nthreads = os.cpu_count() or 1
     os.environ.setdefault("OMP_NUM_THREADS", str(nthreads))
     os.environ.setdefault("OMP_PROC_BIND", "close")
@@ -280,13 +302,17 @@ def cpu_reference_rate(workload: str, steps: int, warmup: int):
     cfl = WORKLOADS[workload][1]
     if warmup:
         U, _ = chk.advance(d, U, cfl, 1e300, warmup)
-    t0 = time.perf_counter()
-    chk.advance(d, U, cfl, 1e300, steps)
-    el = time.perf_counter() - t0
+    secs = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        chk.advance(d, U, cfl, 1e300, steps)
+        secs.append(time.perf_counter() - t0)
+    el = float(np.median(secs))
     rate = d.ncell * steps / el
     cores = chk.max_threads() if hasattr(chk, "max_threads") else (nthreads if kind == "reference" else 1)
     return {"value": rate, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{sample}; {steps} steps after {warmup} warm-up", "seconds": el}
+            "sample": f"{sample} ({d.ncell} cells); {warmup} warm-up step(s), then the median of {repeats} "
+                      f"repeats of {steps} steps", "seconds": el, "cells": d.ncell}
 
 
 def run_reference(args):
@@ -294,12 +320,16 @@ def run_reference(args):
     if rank != 0:
         return
     steps = max(1, args.steps)
-    cb = cpu_reference_rate(args.workload, steps, min(args.warmup, 1))
+    cb = cpu_reference_rate(args.workload, steps, warmup=1, repeats=3)
+    config = {"workload": WORKLOADS[args.workload][0], "parallelism": "cpu-openmp"}
+    if args.workload in ("c0", "c1", "e2"):
+        d, _ = make_workload(args.workload)
+        config.update({"cells": d.ncell, "components": d.nvar})
     line = {
         "impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus,
         "steps": steps, "warmup": args.warmup, "ms_per_step": cb["seconds"] / steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic", "config": {"workload": WORKLOADS[args.workload][0], "parallelism": "cpu-openmp"},
+        "data": "synthetic", "config": config,
         "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
         "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -451,11 +481,32 @@ def run_ours(args):
     alg_bytes = 2 * V * 8 * ncell  # read + write of the state, per sweep launch
     achieved = alg_bytes / avg_sweep_s / 1e9
     peak, peak_src = measured_peaks()
-    traffic, traffic_src = ncu_traffic(args.workload + ("-mixed" if args.precision == "mixed" else ""))
+    pkey = args.workload + ("-mixed" if args.precision == "mixed" else "")
+    traffic, traffic_src = ncu_traffic(pkey)
+    flops_cell, flops_src = ncu_fp64_flops_per_cell(pkey)
+    fp64_peak_flops = fp64_peak()
     sched = "mixed staged sweep (mixed_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
         "staged sweep (staged_a..staged_e)"
     if args.workload in EULER_WORKLOADS:
         sched = "euler_sweep_kernel (fused tile)"
+
+    hbm = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+           "traffic": traffic, "kernel": sched,
+           "note": f"algorithmic {alg_bytes} B per sweep launch (2*V*8*cells); avg sweep "
+                   f"{avg_sweep_s * 1e3:.4f} ms over {sweep['launches']} launches; peak {peak_src} (hbm_gbs)"
+                   + (f"; traffic from {traffic_src}" if traffic_src else "")}
+    fp64 = None
+    if flops_cell and fp64_peak_flops:
+        fa = flops_cell * ncell / avg_sweep_s / 1e12
+        fp = fp64_peak_flops / 1e12
+        fp64 = {"bound": "fp64", "achieved": fa, "peak": fp, "unit": "TFLOP/s", "frac": fa / fp,
+                "kernel": sched,
+                "note": f"{flops_cell:.1f} FP64 operations per cell and sweep (DADD + DMUL + 2 DFMA, ncu, "
+                        f"{flops_src}) x {ncell} cells / avg sweep; peak = DFMA loop on every SM measured "
+                        f"in this run (libdimprobe.so)"}
+    roofline = dict(fp64 if fp64 and fp64["frac"] > hbm["frac"] else hbm)
+    roofline["hbm"] = hbm
+    roofline["fp64"] = fp64
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -467,13 +518,7 @@ def run_ours(args):
             "l2": "flushed between steps" if flush_l2 else "state larger than L2",
             "tiles": "default", "last_dt": float(dts[-1]) if len(dts) else None,
         },
-        "roofline": {
-            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": traffic, "kernel": sched,
-            "note": f"algorithmic {alg_bytes} B per sweep launch (2*V*8*cells); avg sweep "
-                    f"{avg_sweep_s * 1e3:.4f} ms over {sweep['launches']} launches; peak {peak_src}"
-                    + (f"; traffic from {traffic_src}" if traffic_src else ""),
-        },
+        "roofline": roofline,
         "phase_ms": {k: v["ms"] for k, v in prof.items()},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": V * ncell * 8,
                 "d2h_bytes_per_step": V * ncell * 8 + 8},
@@ -485,7 +530,7 @@ def run_ours(args):
         line["precision"] = "mixed"
         line["error_vs_fp64_oracle"] = error_vs_fp64
     if world == 1 and not args.no_cpu:
-        cb = cpu_reference_rate(args.workload, steps=2 if args.workload != "c0" else 20, warmup=0)
+        cb = cpu_reference_rate(args.workload, steps=200 if args.workload == "c0" else 3, warmup=1, repeats=3)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -587,15 +632,14 @@ def run_serving(args):
     # warm-up: kernels loaded and the batch graphs captured
     warm = serve.make_requests(4, 0.0, seed=1000, steps_range=(16, 16), n1d_range=(256, 256),
                                side2d_range=(128, 128))
-    with serve.Server(stream_handle=stream.cuda_stream) as srv:
+    with serve.Server(hbm_budget_bytes=8e9) as srv:
         srv.serve(warm)
     serve.sequential(warm[:1], stream_handle=stream.cuda_stream)
     rows = []
     with ClockSampler(local) as clk:
         for rate in args.c4_rates:
             reqs = serve.make_requests(args.c4_requests, rate, seed=7 + rank)
-            with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8,
-                              stream_handle=stream.cuda_stream) as srv:
+            with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8) as srv:
                 st = srv.serve(reqs)
             sq = serve.sequential(reqs, stream_handle=stream.cuda_stream)
             p50, p99 = st.latency_percentiles()

@@ -98,6 +98,57 @@ class Desc(C.Structure):
         return d
 
 
+class ShockBubbleIC(C.Structure):
+    """dimgpu_ic_shock_bubble."""
+    _fields_ = [("center", C.c_double * 2), ("radius", C.c_double), ("thickness", C.c_double),
+                ("sharpness", C.c_double), ("shock_x", C.c_double), ("zero_below", C.c_double),
+                ("rho_post", C.c_double), ("u_post", C.c_double), ("p_post", C.c_double),
+                ("rho_pre", C.c_double), ("p_pre", C.c_double), ("rho_bubble", C.c_double),
+                ("p_bubble", C.c_double)]
+
+
+class BubbleIC(C.Structure):
+    """dimgpu_ic_bubble."""
+    _fields_ = [("center", C.c_double * 3), ("radius", C.c_double), ("box_lo", C.c_int * 3),
+                ("box_hi", C.c_int * 3)]
+
+
+class BubbleCloudIC(C.Structure):
+    """dimgpu_ic_bubble_cloud."""
+    _fields_ = [("thickness", C.c_double), ("sharpness", C.c_double), ("zero_below", C.c_double),
+                ("pulse_width", C.c_double), ("rho_liquid", C.c_double), ("rho_gas", C.c_double),
+                ("p_ambient", C.c_double), ("p_pulse", C.c_double)]
+
+
+class ServerConfig(C.Structure):
+    """dimgpu_server_config."""
+    _fields_ = [("hbm_budget_bytes", C.c_double), ("dim_share", C.c_double * 3), ("max_slots", C.c_int),
+                ("quantum", C.c_int), ("max_steps_per_solve", C.c_int)]
+
+
+class ServerCounters(C.Structure):
+    """dimgpu_server_counters."""
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("cancelled", C.c_longlong),
+                ("failed", C.c_longlong), ("quanta", C.c_longlong), ("queued", C.c_longlong),
+                ("resident", C.c_int), ("peak_resident", C.c_int), ("peak_bytes", C.c_double)]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_CANCELLED, REQ_FAILED = 0, 1, 2, 3, 4
+
+
+def fill_struct(st: C.Structure, values: dict) -> C.Structure:
+    """Set the fields of a ctypes structure from a dict (sequences for arrays)."""
+    for name, _ in st._fields_:
+        v = values[name]
+        if isinstance(v, (tuple, list)):
+            arr = getattr(st, name)
+            for i, x in enumerate(v):
+                arr[i] = x
+        else:
+            setattr(st, name, v)
+    return st
+
+
 class PhaseTimes(C.Structure):
     _fields_ = [("cfl_ms", C.c_double), ("sweep_ms", C.c_double), ("boundary_ms", C.c_double)]
 

@@ -74,6 +74,23 @@ class Batch:
         self._check(lib().dimgpu_batch_download(self._h, iid, dptr(out), out.size, dptr(dts) if with_dts else None))
         return out, dts[:done]
 
+    def reserve(self, max_cells: int, max_instances: int, max_steps: int) -> None:
+        """Arena mode: device memory for every later add is reserved now, so
+        add / remove allocate and synchronise nothing."""
+        self._check(lib().dimgpu_batch_reserve(self._h, max_cells, max_instances, max_steps))
+
+    def arena_used(self) -> tuple[int, int]:
+        cells, dts = C.c_longlong(), C.c_longlong()
+        self._check(lib().dimgpu_batch_arena_used(self._h, C.byref(cells), C.byref(dts)))
+        return cells.value, dts.value
+
+    def enqueue(self, n: int) -> None:
+        """Enqueue up to n steps without waiting (see wait)."""
+        self._check(lib().dimgpu_batch_enqueue(self._h, n))
+
+    def wait(self) -> None:
+        self._check(lib().dimgpu_batch_wait(self._h))
+
     def set_stream(self, stream_handle: int | None) -> None:
         self._check(lib().dimgpu_batch_set_stream(self._h, C.c_void_p(stream_handle or 0)))
 

@@ -19,14 +19,18 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libdimgpu.so")
+# bench.py's FP64 throughput probe, kept out of the C-ABI library
+PROBE_LIB = os.path.join(HERE, "libdimprobe.so")
+PROBE_SRC = os.path.join(CSRC, "fp64_peak.cu")
 
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
          "-ccbin", "g++", f"-I{os.path.join(ROOT, 'include')}", f"-I{CSRC}"]
 SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "inst_euler.cu", "dimgpu_api.cu",
-           "dimgpu_noalloc.cu", "dimgpu_batch.cu"]
+           "dimgpu_noalloc.cu", "dimgpu_batch.cu", "dimgpu_io.cu", "dimgpu_server.cu"]
 HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h", "dim_batch.cuh", "dim_mixed.h",
+           "dimgpu_validate.h", "dimgpu_session.h", "dim_io.cuh",
            "euler_physics.h", "euler_kernels.cuh"]
 
 
@@ -61,6 +65,12 @@ def build(verbose: bool = False, ptxas_verbose: bool = False) -> str:
         out = subprocess.run(cmd, capture_output=True, text=True)
         if out.returncode != 0:
             raise RuntimeError(f"link failed:\n{out.stdout}\n{out.stderr}")
+    if _mtime(PROBE_LIB) < _mtime(PROBE_SRC):
+        cmd = [NVCC, *ARCH, "-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-shared", PROBE_SRC, "-o", PROBE_LIB,
+               "-lcudart_static", "-ldl", "-lrt", "-lpthread"]
+        out = subprocess.run(cmd, capture_output=True, text=True)
+        if out.returncode != 0:
+            raise RuntimeError(f"nvcc failed on fp64_peak.cu:\n{out.stdout}\n{out.stderr}")
     return LIB
 
 

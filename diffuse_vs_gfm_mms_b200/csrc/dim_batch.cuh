@@ -6,9 +6,12 @@
 // with prefix[i] <= wb < prefix[i+1] (a device table, so membership can
 // change without relaunch geometry changing: a captured CUDA graph stays
 // valid).  Per instance: its Grid, Mats, two state buffers, a dt log and its
-// remaining step count live in a device table of BInst.  All instances share
-// one sweep parity (which of their two buffers is current); an instance that
-// does not run in a step copies its state across so the parity stays right.
+// remaining step count live in a device table of BInst.  Each instance keeps
+// its own buffer parity: `cur` is its current buffer at the start of the
+// step, sweep k of a step reads st[cur ^ (k & 1)] and writes the other one,
+// and an instance that does not run in a step touches neither buffer.  The
+// parity advances in the next step's finalize (by D if the instance ran), so
+// no kernel of a step depends on another instance's progress.
 #pragma once
 
 #include "dim_kernels.cuh"
@@ -30,9 +33,17 @@ __device__ __forceinline__ int batch_find(const long long* __restrict__ prefix, 
 }
 
 // ---- CFL ----------------------------------------------------------------------------
+// Current buffer at the start of this step: the previous step's start
+// buffer, advanced by D sweeps if the instance ran in that step.
+template<int D>
+__device__ __forceinline__ int batch_cur(const BInst& I)
+{
+    return I.run ? (I.cur ^ (D & 1)) : I.cur;
+}
+
 template<int NM, int D>
 __global__ void __launch_bounds__(256) batch_cfl(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                                 int ninst, int parity, double* __restrict__ blockmin)
+                                                 int ninst, double* __restrict__ blockmin)
 {
     __shared__ double red[8];
     const long long total = prefix[ninst];
@@ -44,7 +55,7 @@ __global__ void __launch_bounds__(256) batch_cfl(const BInst* __restrict__ tab, 
         if (I.steps_left > 0 && c < I.g.ncell) {
             State<NM, D> U;
             Prim<NM, D> P;
-            load_cell<NM, D>(I.st[parity], I.g.ncell, c, U);
+            load_cell<NM, D>(I.st[batch_cur<D>(I)], I.g.ncell, c, U);
             if (I.mixed) cons_to_prim_mixed<NM, D>(I.M, U, P);
             else cons_to_prim<NM, D>(I.M, U, P);
             best = cfl_candidate<NM, D>(I.M, U, P, I.g.dx, I.cfl, false);
@@ -61,9 +72,11 @@ __global__ void __launch_bounds__(256) batch_cfl(const BInst* __restrict__ tab, 
     }
 }
 
-// One block per instance (strided): dt = min(dt_max, candidates); decides
-// whether the instance runs this step and logs its dt.
-static __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__ tab, const long long* __restrict__ prefix,
+// One block per instance (strided): advances the instance's buffer parity
+// past the previous step, then dt = min(dt_max, candidates), decides whether
+// the instance runs this step and logs its dt.
+template<int D>
+__global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                       int ninst, const double* __restrict__ blockmin,
                                                       int* __restrict__ err)
 {
@@ -78,6 +91,7 @@ static __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__
             BInst& I = tab[i];
             double m = red[0];
             for (int w = 1; w < 8; ++w) m = dmin(m, red[w]);
+            I.cur = batch_cur<D>(I);
             if (I.steps_left > 0) {
                 const double d = dmin(I.dt_max, m);
                 I.dt = d;
@@ -110,14 +124,14 @@ static __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__
         ls.nl = (int)(I.g.ncell / n);                                                      \
         const StagedItem<DIR> it(I.g, ls, t);                                              \
         const long long q = I.soff + t;                                                    \
-        const double* in = I.st[parity];                                                   \
+        const double* in = I.st[I.cur ^ rel];                                              \
         (void)in;
 
 #define BATCH_LOOP_END }
 
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) batch_a(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                               int ninst, int parity, StagedBufs<NM, D> b)
+                                               int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1) continue;
@@ -135,7 +149,7 @@ __global__ void __launch_bounds__(256) batch_a(const BInst* __restrict__ tab, co
 
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) batch_b(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                               int ninst, int parity, StagedBufs<NM, D> b)
+                                               int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1) continue;
@@ -168,7 +182,7 @@ __global__ void __launch_bounds__(256) batch_b(const BInst* __restrict__ tab, co
 
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) batch_c(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                               int ninst, int parity, StagedBufs<NM, D> b)
+                                               int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1 || I.mixed) continue;  // mixed instances build their face states in batch_d
@@ -199,7 +213,7 @@ __global__ void __launch_bounds__(256) batch_c(const BInst* __restrict__ tab, co
 
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) batch_d(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                               int ninst, int parity, StagedBufs<NM, D> b, int* __restrict__ err)
+                                               int ninst, int rel, StagedBufs<NM, D> b, int* __restrict__ err)
 {
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1 || it.gi >= n - 1) continue;
@@ -226,17 +240,18 @@ __global__ void __launch_bounds__(256) batch_d(const BInst* __restrict__ tab, co
     BATCH_LOOP_END
 }
 
-// Stage E writes the other buffer; instances that do not run this step (or
-// whose line along DIR is a single cell) copy their state across instead.
+// Stage E writes the other buffer; a running instance whose line along DIR
+// is a single cell (no update along that axis) copies its state across.
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256) batch_e(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
-                                               int ninst, int parity, StagedBufs<NM, D> b)
+                                               int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
-    double* out = I.st[1 - parity];
+    if (!I.run) continue;
+    double* out = I.st[I.cur ^ rel ^ 1];
     State<NM, D> U;
     load_cell<NM, D>(in, I.g.ncell, it.cell, U);
-    if (!I.run || n == 1) {
+    if (n == 1) {
         store_cell<NM, D>(out, I.g.ncell, it.cell, U);
         continue;
     }
@@ -258,7 +273,7 @@ __global__ void __launch_bounds__(256) batch_e(const BInst* __restrict__ tab, co
 // batch admits only grids whose fill is order-independent).
 template<int NM, int D>
 __global__ void __launch_bounds__(256) batch_bc(const BInst* __restrict__ tab, const long long* __restrict__ bprefix,
-                                                int ninst, int parity)
+                                                int ninst, int rel)
 {
     const long long total = bprefix[ninst];
     for (long long wb = blockIdx.x; wb < total; wb += gridDim.x) {
@@ -292,7 +307,7 @@ __global__ void __launch_bounds__(256) batch_bc(const BInst* __restrict__ tab, c
         idx[a] = side ? I.g.N[a] - 1 : 0;
         long long linear = 0;
         for (int bb = 0; bb < D; ++bb) linear += (long long)idx[bb] * I.g.stride[bb];
-        bc_cell<NM, D>(I.g, I.M, I.st[parity], idx, linear);
+        bc_cell<NM, D>(I.g, I.M, I.st[I.cur ^ rel], idx, linear);
     }
 }
 
@@ -300,7 +315,7 @@ __global__ void __launch_bounds__(256) batch_bc(const BInst* __restrict__ tab, c
 
 
 template<int NM, int D>
-cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s)
+cudaError_t batch_step(const BatchLaunch& L, cudaStream_t s)
 {
     StagedBufs<NM, D> b;
     b.cap = L.cap;
@@ -314,17 +329,17 @@ cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s)
     b.PLS = p; p += kPrimVars(NM, D) * L.cap;
     b.PRS = p; p += kPrimVars(NM, D) * L.cap;
     b.F = p;
-    batch_cfl<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, parity, L.blockmin);
-    batch_finalize<<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, L.blockmin, L.err);
-    int par = parity;
+    batch_cfl<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, L.blockmin);
+    batch_finalize<D><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, L.blockmin, L.err);
+    // sweep k reads st[cur ^ (k & 1)]; the boundary fill after it works on the
+    // buffer it wrote, st[cur ^ (k & 1) ^ 1]
 #define BATCH_DIR(DIR)                                                                                   \
-    batch_a<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, par, b);                   \
-    batch_b<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, par, b);                   \
-    batch_c<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, par, b);                   \
-    batch_d<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, par, b, L.err);            \
-    batch_e<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, par, b);                   \
-    par = 1 - par;                                                                                       \
-    batch_bc<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.bc_prefix, L.ninst, par);
+    batch_a<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
+    batch_b<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
+    batch_c<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
+    batch_d<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b, L.err);        \
+    batch_e<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
+    batch_bc<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.bc_prefix, L.ninst, (DIR & 1) ^ 1);
     BATCH_DIR(0)
     if constexpr (D >= 2) { BATCH_DIR(1) }
     if constexpr (D >= 3) { BATCH_DIR(2) }
@@ -333,8 +348,8 @@ cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s)
 }
 
 #define DIMGPU_INSTANTIATE_BATCH(NM)                                                        \
-    template cudaError_t batch_step<NM, 1>(const BatchLaunch&, int, cudaStream_t);          \
-    template cudaError_t batch_step<NM, 2>(const BatchLaunch&, int, cudaStream_t);          \
-    template cudaError_t batch_step<NM, 3>(const BatchLaunch&, int, cudaStream_t);
+    template cudaError_t batch_step<NM, 1>(const BatchLaunch&, cudaStream_t);               \
+    template cudaError_t batch_step<NM, 2>(const BatchLaunch&, cudaStream_t);               \
+    template cudaError_t batch_step<NM, 3>(const BatchLaunch&, cudaStream_t);
 
 }  // namespace dimgpu

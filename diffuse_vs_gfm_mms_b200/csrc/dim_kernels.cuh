@@ -141,7 +141,7 @@ __host__ __device__ constexpr int kSweepSmemVars(int nm, int d) { return kStateV
 // memory, so every stage is separated by one __syncthreads.
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, 2) sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
-                                                    Grid g, Mats M, int T, int W, int ntile, int ngx,
+                                                    __grid_constant__ const Grid g, __grid_constant__ const Mats M, int T, int W, int ntile, int ngx,
                                                     const double* __restrict__ dtp, int* __restrict__ err)
 {
     extern __shared__ double sm[];
@@ -405,6 +405,12 @@ struct StagedItem {
     }
 };
 
+// Resident blocks of 256 threads per SM that the staged kernels are compiled
+// for (their register budget: 65536 / (256 * blocks)).
+#ifndef DIMGPU_STAGED_MINB
+#define DIMGPU_STAGED_MINB 2
+#endif
+
 // Optional CFL reduction fused into stage A of the first sweep of a step:
 // stage A recovers every cell's primitive from the very state the CFL
 // minimum is taken over, so the candidate costs one sound speed, not a
@@ -433,7 +439,7 @@ __device__ __forceinline__ void fused_cfl_reduce(double best, const FusedCfl& c)
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) staged_a(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b, FusedCfl fc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -454,7 +460,7 @@ __global__ void __launch_bounds__(256) staged_a(const double* __restrict__ in, G
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) staged_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -483,7 +489,7 @@ __global__ void __launch_bounds__(256) staged_b(const double* __restrict__ in, G
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) staged_c(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_c(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -515,7 +521,7 @@ __global__ void __launch_bounds__(256) staged_c(const double* __restrict__ in, G
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) staged_d(Grid g, Mats M, LineSet ls, StagedBufs<NM, D> b,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_d(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 int* __restrict__ err)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -534,8 +540,8 @@ __global__ void __launch_bounds__(256) staged_d(Grid g, Mats M, LineSet ls, Stag
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) staged_e(const double* __restrict__ in, double* __restrict__ out, Grid g,
-                                                Mats M, LineSet ls, StagedBufs<NM, D> b,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_e(const double* __restrict__ in, double* __restrict__ out, __grid_constant__ const Grid g,
+                                                __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 const double* __restrict__ dtp)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -566,7 +572,7 @@ __global__ void __launch_bounds__(256) staged_e(const double* __restrict__ in, d
 // so the face states never reach HBM.  Scratch: P, ck, Pe, Ph and the face
 // records, at the staged positions.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                StagedBufs<NM, D> b, FusedCfl fc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -592,7 +598,7 @@ __global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, Gr
 // cut the mixed step's time on a B200 by 2.5 % (2D shock-bubble 1024x512)
 // and 1.2 % (3D bubble cloud 256^3).
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -639,7 +645,7 @@ __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const 
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in, Grid g, Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                    StagedBufs<NM, D> b, int* __restrict__ err)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -681,7 +687,7 @@ __device__ __forceinline__ double warp_min(double v)
 }
 
 template<int NM, int D>
-__global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st, Grid g, Mats M, double cfl,
+__global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, double cfl,
                                                   int unsplit, int mixed, double* __restrict__ blockmin)
 {
     __shared__ double red[32];
@@ -821,7 +827,7 @@ __device__ void bc_cell(const Grid& g, const Mats& M, double* st, const int* idx
 // idx[a] == (side ? N[a]-1 : 0) whose lower axes b < a are interior, so
 // every boundary cell is visited exactly once.
 template<int NM, int D>
-__global__ void __launch_bounds__(256) bc_kernel(double* st, Grid g, Mats M, long long plane0, long long plane1,
+__global__ void __launch_bounds__(256) bc_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, long long plane0, long long plane1,
                                                  long long plane2)
 {
     const long long count[3] = {plane0, plane1, plane2};
@@ -850,7 +856,7 @@ __global__ void __launch_bounds__(256) bc_kernel(double* st, Grid g, Mats M, lon
 
 // The reference's literal serial order, for grids where it matters.
 template<int NM, int D>
-__global__ void bc_serial_kernel(double* st, Grid g, Mats M)
+__global__ void bc_serial_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (long long linear = 0; linear < g.ncell; ++linear) {
@@ -868,7 +874,7 @@ __global__ void bc_serial_kernel(double* st, Grid g, Mats M)
 // ---- unsplit accumulation (src/dim/solver/advance_step.hpp:77-101) -------------
 template<int NM, int D>
 __global__ void __launch_bounds__(256) accumulate_kernel(double* __restrict__ acc, const double* __restrict__ dir_state,
-                                                         const double* __restrict__ base, Grid g, Mats M)
+                                                         const double* __restrict__ base, __grid_constant__ const Grid g, __grid_constant__ const Mats M)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= g.ncell) return;
@@ -890,7 +896,7 @@ __global__ void __launch_bounds__(256) accumulate_kernel(double* __restrict__ ac
 // ---- conservation totals (compute_dim_conservation_totals,
 // src/app/io/conservation_report.hpp:188-218): per-block partial sums ------------
 template<int NM, int D>
-__global__ void __launch_bounds__(256) totals_kernel(const double* __restrict__ st, Grid g, double volume,
+__global__ void __launch_bounds__(256) totals_kernel(const double* __restrict__ st, __grid_constant__ const Grid g, double volume,
                                                      double* __restrict__ partial)
 {
     constexpr int NV = NM + 1 + D + 1;
@@ -1168,7 +1174,7 @@ cudaError_t launch_totals(const Grid& g, const double* state, double volume, dou
 // area * (F(right end cell) - F(left end cell)) with the physical normal flux
 // of each end cell's own state; per-block partial sums ----------------------------
 template<int NM, int D>
-__global__ void __launch_bounds__(256) boundary_flux_kernel(const double* __restrict__ st, Grid g, Mats M,
+__global__ void __launch_bounds__(256) boundary_flux_kernel(const double* __restrict__ st, __grid_constant__ const Grid g, __grid_constant__ const Mats M,
                                                             long long lines0, long long lines1, double area0,
                                                             double area1, double area2,
                                                             double* __restrict__ partial)

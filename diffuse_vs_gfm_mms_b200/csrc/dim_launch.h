@@ -113,6 +113,7 @@ struct BInst {
     int steps_left;     // steps still to run
     int steps_done;     // steps run so far
     int run;            // runs in the current step (set by the finalize kernel)
+    int cur;            // current buffer at the start of the step that last ran finalize
     int mixed;          // DIMGPU_PRECISION_MIXED: mixed_b / mixed_cd arithmetic
     double cfl, dt_max;
     double dt;          // dt of the current step
@@ -134,7 +135,7 @@ struct BatchLaunch {
 // One time step of every running instance: per-instance CFL, the staged
 // sweeps and boundary fills, with a persistent grid of L.grid CTAs.
 template<int NM, int D>
-cudaError_t batch_step(const BatchLaunch& L, int parity, cudaStream_t s);
+cudaError_t batch_step(const BatchLaunch& L, cudaStream_t s);
 
 int sweep_smem_doubles(int nmat, int dim);
 

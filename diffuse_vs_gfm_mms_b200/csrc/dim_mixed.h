@@ -108,8 +108,9 @@ DHD double pressure_closed_form(const Mats& M, double rho_total, double e, const
 
 // cons_to_prim (primitives.hpp:111-162) with the closed-form recovery.
 template<int NM, int D>
-DNI void cons_to_prim_mixed(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+DNI Prim<NM, D> cons_to_prim_mixed_v(const Mats& M, State<NM, D> U)
 {
+    Prim<NM, D> P;
     full_alpha<NM, D>(U, P.alpha);
     sanitise_alpha<NM>(P.alpha, 1e-12);
     double rho_total = 0.0;
@@ -130,6 +131,13 @@ DNI void cons_to_prim_mixed(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P
     const double kinetic = 0.5 * rho_total * velocity_squared;
     const double internal_energy = safe_div(finite_or(U.E, kinetic) - kinetic, rho_total);
     P.p = dmax(pressure_closed_form<NM>(M, rho_total, internal_energy, P.alpha, P.rho), 1e-12);
+    return P;
+}
+
+template<int NM, int D>
+DHD void cons_to_prim_mixed(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+{
+    P = cons_to_prim_mixed_v<NM, D>(M, U);
 }
 
 // Stage A of the mixed step (stage_a with the closed-form recovery).

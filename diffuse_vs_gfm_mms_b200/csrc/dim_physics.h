@@ -25,7 +25,12 @@
 // DHD: small helpers, inlined.  DNI: the large routines every sweep calls at
 // many sites (pressure recovery, cons_to_prim, prim_to_cons, repair_state,
 // the generic sound speed), kept as single out-of-line copies on the device
-// so the sweep kernel's code fits the instruction cache.
+// so the sweep kernel's code fits the instruction cache.  The out-of-line
+// copies take and return their records by value (the *_v functions): a
+// record passed by reference or pointer must live in addressable (local)
+// memory, which turns every call into local stores and loads; by value it
+// stays in registers.  Inline wrappers with the by-reference signatures sit
+// in front of them.
 #ifdef __CUDACC__
 #define DHD __host__ __device__ __forceinline__
 #define DNI __host__ __device__ __noinline__
@@ -186,10 +191,30 @@ struct MixtureBisection {
     }
 };
 
+// Volume fractions and material densities of a mixture state, passed by value.
 template<int NM>
-DNI double pressure_from_internal_energy(const Mats& M, double rho_total, double e,
-                                         const double* alpha, const double* rho)
+struct MixVec {
+    double alpha[NM];
+    double rho[NM];
+};
+
+template<int NM>
+DHD MixVec<NM> mix_of(const double* alpha, const double* rho)
 {
+    MixVec<NM> x;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) {
+        x.alpha[k] = alpha[k];
+        x.rho[k] = rho[k];
+    }
+    return x;
+}
+
+template<int NM>
+DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, double e, MixVec<NM> x)
+{
+    const double* alpha = x.alpha;
+    const double* rho = x.rho;
     rho_total = clamp_min(rho_total);
     e = finite_or(e);
     const double target = finite_or(rho_total * e);
@@ -222,15 +247,23 @@ DNI double pressure_from_internal_energy(const Mats& M, double rho_total, double
 
     // Certain-decision bracket (see the comment above MixtureBisection).
     constexpr double kRel = 256.0 * 1.1102230246251565e-16;
+    constexpr double kInvOneMinusRel = 1.0 / (1.0 - kRel);
+    constexpr double kInvOnePlusRel = 1.0 / (1.0 + kRel);
     bool fast = fin(A) && fin(B) && A > 1e-200 && (B + fabs(target)) < 1e290;
     double P_lo = 0.0, P_hi = 0.0, P_fin = 0.0;
     if (fast) {
+        // One division: the bounds are products with 1/A.  Each product is
+        // within 4u of the quotient it replaces (the rounding of 1/A, of the
+        // constant 1/(1 -+ kRel) and of two products), far inside the 1e-13
+        // relative widening that follows, so the bounds stay outer bounds;
+        // P_fin only guards against overflow and needs no precision.
+        const double rA = 1.0 / A;
         const double slack = kRel * (B + fabs(target));
-        P_hi = (thresh + target - B + slack) / (A * (1.0 - kRel));
-        P_lo = (target - B - thresh - slack) / (A * (1.0 + kRel));
+        P_hi = (thresh + target - B + slack) * (rA * kInvOneMinusRel);
+        P_lo = (target - B - thresh - slack) * (rA * kInvOnePlusRel);
         P_hi = P_hi + fabs(P_hi) * 1e-13 + 1e-300;
         P_lo = P_lo - fabs(P_lo) * 1e-13 - 1e-300;
-        P_fin = 1e290 / A;
+        P_fin = 1e290 * rA;
         fast = fin(P_hi) && fin(P_lo);
     }
     // status: -1 certainly f < -thresh, +1 certainly f > thresh, 0 unknown
@@ -310,6 +343,13 @@ DNI double pressure_from_internal_energy(const Mats& M, double rho_total, double
     return clamp_min(0.5 * (lo + hi));
 }
 
+template<int NM>
+DHD double pressure_from_internal_energy(const Mats& M, double rho_total, double e, const double* alpha,
+                                         const double* rho)
+{
+    return pressure_from_internal_energy_v<NM>(M, rho_total, e, mix_of<NM>(alpha, rho));
+}
+
 // MixtureEOS::mixture_sound_speed, src/dim/eos.hpp:195-221
 template<int NM>
 DHD double mixture_sound_speed(const Mats& M, double rho_total, double p, const double* alpha,
@@ -329,9 +369,10 @@ DHD double mixture_sound_speed(const Mats& M, double rho_total, double p, const 
 
 // MixtureEOS::generic_mixture_sound_speed, src/dim/eos.hpp:223-275
 template<int NM>
-DNI double generic_mixture_sound_speed(const Mats& M, double rho_total, double p,
-                                       const double* alpha, const double* rho)
+DNI double generic_mixture_sound_speed_v(const Mats& M, double rho_total, double p, MixVec<NM> x)
 {
+    const double* alpha = x.alpha;
+    const double* rho = x.rho;
     if (M.lambda_model == 0) return mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
     double sound_speed[NM], xi[NM];
     double xi_mix = 0.0, inverse_sound_sum = 0.0;
@@ -356,6 +397,13 @@ DNI double generic_mixture_sound_speed(const Mats& M, double rho_total, double p
         rho_c_squared += lambda_k * alpha_k * xi[k] * sound_speed[k] * sound_speed[k] / xi_mix;
     }
     return sqrt(dmax(rho_c_squared / clamp_min(rho_total), 1e-14));
+}
+
+template<int NM>
+DHD double generic_mixture_sound_speed(const Mats& M, double rho_total, double p, const double* alpha,
+                                       const double* rho)
+{
+    return generic_mixture_sound_speed_v<NM>(M, rho_total, p, mix_of<NM>(alpha, rho));
 }
 
 // ---- src/dim/primitives.hpp ----------------------------------------------------
@@ -407,8 +455,9 @@ DHD double total_density(const State<NM, D>& U)
 
 // cons_to_prim, primitives.hpp:111-162
 template<int NM, int D>
-DNI void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+DNI Prim<NM, D> cons_to_prim_v(const Mats& M, State<NM, D> U)
 {
+    Prim<NM, D> P;
     full_alpha<NM, D>(U, P.alpha);
     sanitise_alpha<NM>(P.alpha, 1e-12);
     double rho_total = 0.0;
@@ -429,13 +478,21 @@ DNI void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
     const double kinetic = 0.5 * rho_total * velocity_squared;
     const double internal_energy = safe_div(finite_or(U.E, kinetic) - kinetic, rho_total);
     P.p = dmax(pressure_from_internal_energy<NM>(M, rho_total, internal_energy, P.alpha, P.rho), 1e-12);
+    return P;
+}
+
+template<int NM, int D>
+DHD void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
+{
+    P = cons_to_prim_v<NM, D>(M, U);
 }
 
 // prim_to_cons, primitives.hpp:165-212 (internal_energy_from_pressure,
 // src/dim/eos.hpp:146-166, inlined)
 template<int NM, int D>
-DNI void prim_to_cons(const Mats& M, Prim<NM, D> P, State<NM, D>& U)
+DNI State<NM, D> prim_to_cons_v(const Mats& M, Prim<NM, D> P)
 {
+    State<NM, D> U;
     sanitise_alpha<NM>(P.alpha, 1e-12);
     double rho_total = 0.0;
 #pragma unroll
@@ -456,6 +513,13 @@ DNI void prim_to_cons(const Mats& M, Prim<NM, D> P, State<NM, D>& U)
     U.E = rho_total * ie + 0.5 * rho_total * velocity_squared;
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) U.a[k] = P.alpha[k];
+    return U;
+}
+
+template<int NM, int D>
+DHD void prim_to_cons(const Mats& M, const Prim<NM, D>& P, State<NM, D>& U)
+{
+    U = prim_to_cons_v<NM, D>(M, P);
 }
 
 // Material sound speeds at a primitive's (rho_k, p) with the floors that
@@ -529,7 +593,7 @@ DHD void alpha_rhs_coefficients(const Mats& M, const Prim<NM, D>& P, const doubl
 
 // repair_state, primitives.hpp:325-457.
 template<int NM, int D>
-DNI void repair_state(const Mats& M, State<NM, D>& U)
+DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
 {
     const double mass_floor = 1e-12, p_floor = 1e-12, inactive_alpha_floor = 1e-10;
 #pragma unroll
@@ -629,7 +693,7 @@ DNI void repair_state(const Mats& M, State<NM, D>& U)
         ub = ub * (1.0 + 1e-12) + 1e-290;
         if (fin(ub) && E >= ub) {
             U.E = E;
-            return;
+            return U;
         }
     }
     double velocity_squared = 0.0;
@@ -647,6 +711,13 @@ DNI void repair_state(const Mats& M, State<NM, D>& U)
     const double kinetic = 0.5 * rho_total * velocity_squared;
     const double minimum_internal = mixture_ie_density<NM>(M, p_floor, alpha_full, rho_material);
     U.E = dmax(E, kinetic + minimum_internal);
+    return U;
+}
+
+template<int NM, int D>
+DHD void repair_state(const Mats& M, State<NM, D>& U)
+{
+    U = repair_state_v<NM, D>(M, U);
 }
 
 // ---- src/dim/reconstruction/muscl.hpp -----------------------------------------

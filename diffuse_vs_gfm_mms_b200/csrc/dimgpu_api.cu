@@ -10,6 +10,7 @@
 
 #include "dim_launch.h"
 #include "dimgpu.h"
+#include "dimgpu_session.h"
 #include "dimgpu_validate.h"
 
 using namespace dimgpu;
@@ -112,37 +113,10 @@ int staged_scratch_doubles(int nmat, int dim)
 
 void set_sessionless_error(const std::string& msg) { g_err = msg; }
 
+int session_fail(dimgpu_session* s, int code, const std::string& msg) { return fail(s ? &s->msg : nullptr, code, msg); }
+
 }  // namespace dimgpu
 
-struct dimgpu_session {
-    dimgpu_desc desc{};
-    Mats M{};
-    Grid g{};
-    int V = 0;
-    long long ncell = 0;
-    double* buf[3] = {nullptr, nullptr, nullptr};
-    int cur = 0;
-    double* blockmin = nullptr;
-    double* dt = nullptr;
-    double* hist = nullptr;
-    double* partial = nullptr;
-    int* err = nullptr;
-    cudaStream_t own_stream = nullptr;
-    cudaStream_t stream = nullptr;
-    Tile tile[3] = {{128, 1}, {64, 4}, {64, 4}};
-    int schedule[3] = {DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED};
-    double* staged = nullptr;  // scratch of the staged schedule (allocated on first use)
-    unsigned long long* cfl_slot = nullptr;  // fused CFL minimum (bit pattern of a double)
-    long long staged_cap = 0;
-    std::string msg;
-    // profiling
-    bool profiling = false;
-    struct Rec { int kind; cudaEvent_t a, b; };
-    std::vector<Rec> recs;
-    std::vector<cudaEvent_t> pool;
-    double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    int pending = 0;  // steps enqueued since the last collection
-};
 
 namespace {
 
@@ -394,6 +368,10 @@ cudaError_t run_step(dimgpu_session* s, double cfl, double dt_max, double* hist)
 }
 
 }  // namespace
+
+namespace dimgpu {
+int session_cuda_fail(dimgpu_session* s, cudaError_t e, const char* what) { return cuda_fail(s, e, what); }
+}  // namespace dimgpu
 
 extern "C" {
 

@@ -23,7 +23,7 @@ using namespace dimgpu;
 
 namespace {
 
-constexpr int kGraphSteps = 8;  // steps per captured graph (even: parity returns for any dim)
+constexpr int kGraphSteps = 8;  // steps per captured graph
 
 struct HostInst {
     int id;
@@ -33,6 +33,56 @@ struct HostInst {
     long long nbc;        // boundary cells
     int steps_total;
     int steps_left;       // host mirror (exact: every run advances min(n, left))
+    long long cell_off;   // arena mode: first cell of its range (scratch items and state)
+    long long dt_off;     // arena mode: first entry of its dt log range
+};
+
+// First-fit allocator of ranges of [0, capacity): the arena mode's cells and
+// dt-log entries.  Freed ranges merge with their neighbours.
+class RangeAlloc {
+public:
+    void reset(long long cap)
+    {
+        free_.clear();
+        if (cap > 0) free_[0] = cap;
+        used_ = 0;
+    }
+    long long alloc(long long n)
+    {
+        if (n <= 0) n = 1;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < n) continue;
+            const long long off = it->first, len = it->second;
+            free_.erase(it);
+            if (len > n) free_[off + n] = len - n;
+            used_ += n;
+            return off;
+        }
+        return -1;
+    }
+    void release(long long off, long long n)
+    {
+        if (n <= 0) n = 1;
+        used_ -= n;
+        auto it = free_.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    long long used() const { return used_; }
+
+private:
+    std::map<long long, long long> free_;
+    long long used_ = 0;
 };
 
 long long boundary_cells(const dimgpu_desc& d)
@@ -56,7 +106,6 @@ struct dimgpu_batch {
     int nmat = 0, dim = 0;
     std::vector<HostInst> inst;
     int next_id = 1;
-    int parity = 0;
     bool dirty = true;      // tables must be rebuilt before the next step
     // device
     BInst* tab = nullptr;
@@ -69,8 +118,15 @@ struct dimgpu_batch {
     int grid = 148 * 4;
     cudaStream_t stream = nullptr;
     cudaStream_t own_stream = nullptr;
-    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // by start parity
+    cudaGraphExec_t graph = nullptr;
     std::string msg;
+    // arena mode (dimgpu_batch_reserve): everything allocated once
+    bool arena = false;
+    double* st_arena[2] = {nullptr, nullptr};
+    double* dt_arena = nullptr;
+    RangeAlloc cells, dts;
+    BInst* tab_pinned = nullptr;           // host staging of the tables
+    long long* prefix_pinned = nullptr;    // cell prefix, then bc prefix
 };
 
 namespace {
@@ -90,10 +146,8 @@ int bcuda(dimgpu_batch* b, cudaError_t e, const char* what)
 
 void drop_graphs(dimgpu_batch* b)
 {
-    for (auto& g : b->graph) {
-        if (g) cudaGraphExecDestroy(g);
-        g = nullptr;
-    }
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
 }
 
 template<class T>
@@ -110,84 +164,118 @@ cudaError_t grow(T** p, long long* cap, long long need)
     return e;
 }
 
-// Pull the device-side counters of the current members into the host mirror.
-cudaError_t pull_counters(dimgpu_batch* b)
+// The device-table entry of an instance as the device holds it after the
+// steps enqueued so far: steps_done / steps_left from the host mirror;
+// run = whether it ran in the last step enqueued; cur = its buffer at the
+// start of that step (every instance starts in buffer 0 and a step moves it
+// by D sweeps).
+void sync_mirror(const dimgpu_batch* b, HostInst& h)
 {
-    if (b->inst.empty() || !b->tab || b->dirty) return cudaSuccess;
-    std::vector<BInst> dev(b->inst.size());
-    cudaError_t e = cudaMemcpyAsync(dev.data(), b->tab, sizeof(BInst) * dev.size(), cudaMemcpyDeviceToHost, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) return e;
-    for (size_t i = 0; i < dev.size(); ++i) {
-        b->inst[i].dev.steps_left = dev[i].steps_left;
-        b->inst[i].dev.steps_done = dev[i].steps_done;
-        b->inst[i].dev.run = dev[i].run;
-        b->inst[i].dev.dt = dev[i].dt;
-    }
-    return cudaSuccess;
+    const int done = h.steps_total - h.steps_left;
+    h.dev.steps_done = done;
+    h.dev.steps_left = h.steps_left;
+    const int start = done - (h.dev.run ? 1 : 0);
+    h.dev.cur = (int)(((long long)start * b->dim) & 1);
 }
 
-// Rebuild the device tables (and grow the scratch) for the current members.
-// Tables are padded to a capacity C (entries past the members have no work
-// and no steps), and every launch is given C, so a captured graph stays valid
-// across membership changes until a table or the scratch has to grow.
+// The buffer that holds an instance's state after the steps enqueued so far.
+int current_buffer(const dimgpu_batch* b, const HostInst& h)
+{
+    const long long done = h.steps_total - h.steps_left;
+    return (int)((done * b->dim) & 1);
+}
+
+// Rebuild the device tables (and, outside arena mode, grow the scratch) for
+// the current members.  Tables are padded to a capacity C (entries past the
+// members have no work and no steps), and every launch is given C, so a
+// captured graph stays valid across membership changes until a table or the
+// scratch has to grow — which never happens in arena mode.
 cudaError_t rebuild(dimgpu_batch* b)
 {
     const int n = (int)b->inst.size();
     long long items = 0, cells_blocks = 0;
     for (int i = 0; i < n; ++i) {
-        b->inst[i].dev.soff = items;
-        items += b->inst[i].ncell;
+        if (b->arena) {
+            b->inst[i].dev.soff = b->inst[i].cell_off;
+        }
+        else {
+            b->inst[i].dev.soff = items;
+            items += b->inst[i].ncell;
+        }
         cells_blocks += (b->inst[i].ncell + 255) / 256;
+        sync_mirror(b, b->inst[i]);
     }
-    const int nrec = staged_scratch_doubles(b->nmat, b->dim);
-    // A captured graph bakes in the launch arguments (buffer addresses and
-    // the scratch capacity that strides every record): drop it whenever any
-    // of them changes.  An address alone is not enough, since a regrown
-    // buffer can come back at the address of the one it replaces.
-    const long long caps_before[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
-    const void* before[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
-    cudaError_t e = grow(&b->scratch, &b->scratch_cap, std::max<long long>(items, 1) * nrec);
-    if (e == cudaSuccess) e = grow(&b->blockmin, &b->blockmin_cap, std::max<long long>(cells_blocks, 1));
-    if (e == cudaSuccess && (n > b->tab_cap || !b->tab)) {
-        const long long cap = std::max<long long>(std::max<long long>(16, n), b->tab_cap * 2);
-        cudaFree(b->tab);
-        cudaFree(b->cell_prefix);
-        cudaFree(b->bc_prefix);
-        b->tab = nullptr;
-        b->cell_prefix = b->bc_prefix = nullptr;
-        e = cudaMalloc(&b->tab, sizeof(BInst) * (size_t)cap);
-        if (e == cudaSuccess) e = cudaMalloc(&b->cell_prefix, sizeof(long long) * (size_t)(cap + 1));
-        if (e == cudaSuccess) e = cudaMalloc(&b->bc_prefix, sizeof(long long) * (size_t)(cap + 1));
-        b->tab_cap = e == cudaSuccess ? cap : 0;
+    cudaError_t e = cudaSuccess;
+    if (!b->arena) {
+        const int nrec = staged_scratch_doubles(b->nmat, b->dim);
+        // A captured graph bakes in the launch arguments (buffer addresses and
+        // the scratch capacity that strides every record): drop it whenever any
+        // of them changes.  An address alone is not enough, since a regrown
+        // buffer can come back at the address of the one it replaces.
+        const long long caps_before[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
+        const void* before[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
+        e = grow(&b->scratch, &b->scratch_cap, std::max<long long>(items, 1) * nrec);
+        if (e == cudaSuccess) e = grow(&b->blockmin, &b->blockmin_cap, std::max<long long>(cells_blocks, 1));
+        if (e == cudaSuccess && (n > b->tab_cap || !b->tab)) {
+            const long long cap = std::max<long long>(std::max<long long>(16, n), b->tab_cap * 2);
+            cudaFree(b->tab);
+            cudaFree(b->cell_prefix);
+            cudaFree(b->bc_prefix);
+            b->tab = nullptr;
+            b->cell_prefix = b->bc_prefix = nullptr;
+            e = cudaMalloc(&b->tab, sizeof(BInst) * (size_t)cap);
+            if (e == cudaSuccess) e = cudaMalloc(&b->cell_prefix, sizeof(long long) * (size_t)(cap + 1));
+            if (e == cudaSuccess) e = cudaMalloc(&b->bc_prefix, sizeof(long long) * (size_t)(cap + 1));
+            b->tab_cap = e == cudaSuccess ? cap : 0;
+        }
+        if (e != cudaSuccess) return e;
+        const void* after[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
+        const long long caps_after[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
+        if (std::memcmp(before, after, sizeof before) != 0 ||
+            std::memcmp(caps_before, caps_after, sizeof caps_before) != 0)
+            drop_graphs(b);
     }
-    if (e != cudaSuccess) return e;
-    const void* after[5] = {b->scratch, b->blockmin, b->tab, b->cell_prefix, b->bc_prefix};
-    const long long caps_after[3] = {b->scratch_cap, b->blockmin_cap, b->tab_cap};
-    if (std::memcmp(before, after, sizeof before) != 0 || std::memcmp(caps_before, caps_after, sizeof caps_before) != 0)
-        drop_graphs(b);
     const long long C = b->tab_cap;
-    std::vector<BInst> dev((size_t)C);
-    std::memset(dev.data(), 0, sizeof(BInst) * (size_t)C);
-    std::vector<long long> cp((size_t)C + 1, 0), bp((size_t)C + 1, 0);
+    std::vector<BInst> dev_v;
+    std::vector<long long> pre_v;
+    BInst* dev;
+    long long* cp;
+    if (b->arena) {
+        dev = b->tab_pinned;
+        cp = b->prefix_pinned;
+    }
+    else {
+        dev_v.resize((size_t)C);
+        pre_v.resize(2 * (size_t)(C + 1));
+        dev = dev_v.data();
+        cp = pre_v.data();
+    }
+    long long* bp = cp + (C + 1);
+    std::memset(dev, 0, sizeof(BInst) * (size_t)C);
+    cp[0] = bp[0] = 0;
     for (long long i = 0; i < C; ++i) {
         long long cb = 0, bb = 0;
         if (i < n) {
-            dev[i] = b->inst[i].dev;
-            cb = (b->inst[i].ncell + 255) / 256;
-            bb = (b->inst[i].nbc + 255) / 256;
+            dev[i] = b->inst[(size_t)i].dev;
+            cb = (b->inst[(size_t)i].ncell + 255) / 256;
+            bb = (b->inst[(size_t)i].nbc + 255) / 256;
         }
         cp[i + 1] = cp[i] + cb;
         bp[i + 1] = bp[i] + bb;
     }
-    e = cudaMemcpyAsync(b->tab, dev.data(), sizeof(BInst) * (size_t)C, cudaMemcpyHostToDevice, b->stream);
+    // Arena mode: the tables are staged in pinned memory, so the copies are
+    // asynchronous; the host writes the staging again only after the steps
+    // that read it have completed (a caller waits for every enqueued step
+    // before it changes the membership again).  Otherwise: pageable staging
+    // and a synchronisation.
+    e = cudaMemcpyAsync(b->tab, dev, sizeof(BInst) * (size_t)C, cudaMemcpyHostToDevice, b->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->cell_prefix, cp.data(), sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
+        e = cudaMemcpyAsync(b->cell_prefix, cp, sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
                             b->stream);
     if (e == cudaSuccess)
-        e = cudaMemcpyAsync(b->bc_prefix, bp.data(), sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
+        e = cudaMemcpyAsync(b->bc_prefix, bp, sizeof(long long) * (size_t)(C + 1), cudaMemcpyHostToDevice,
                             b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    if (e == cudaSuccess && !b->arena) e = cudaStreamSynchronize(b->stream);
     if (e != cudaSuccess) return e;
     b->dirty = false;
     return cudaSuccess;
@@ -208,12 +296,12 @@ BatchLaunch launch_args(dimgpu_batch* b)
     return L;
 }
 
-cudaError_t one_step(dimgpu_batch* b, const BatchLaunch& L, int parity)
+cudaError_t one_step(dimgpu_batch* b, const BatchLaunch& L)
 {
     cudaError_t e = cudaErrorInvalidValue;
     switch (b->nmat * 10 + b->dim) {
 #define BATCH_CASE(NM, D) \
-        case NM * 10 + D: e = batch_step<NM, D>(L, parity, b->stream); break;
+        case NM * 10 + D: e = batch_step<NM, D>(L, b->stream); break;
         BATCH_CASE(1, 1) BATCH_CASE(1, 2) BATCH_CASE(1, 3)
         BATCH_CASE(2, 1) BATCH_CASE(2, 2) BATCH_CASE(2, 3)
         BATCH_CASE(3, 1) BATCH_CASE(3, 2) BATCH_CASE(3, 3)
@@ -222,6 +310,20 @@ cudaError_t one_step(dimgpu_batch* b, const BatchLaunch& L, int parity)
         default: break;
     }
     return e;
+}
+
+void free_instance(dimgpu_batch* b, HostInst& h)
+{
+    if (b->arena) {
+        if (h.cell_off >= 0) b->cells.release(h.cell_off, h.ncell);
+        if (h.dt_off >= 0) b->dts.release(h.dt_off, std::max(h.steps_total, 1));
+        h.cell_off = h.dt_off = -1;
+    }
+    else {
+        cudaFree(h.dev.st[0]);
+        cudaFree(h.dev.st[1]);
+        cudaFree(h.dev.dtlog);
+    }
 }
 
 }  // namespace
@@ -254,16 +356,63 @@ int dimgpu_batch_create(int nmat, int dim, dimgpu_batch** out)
     return DIMGPU_OK;
 }
 
+int dimgpu_batch_reserve(dimgpu_batch* b, long long max_cells, int max_instances, long long max_steps)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    if (!b->inst.empty() || b->arena)
+        return bfail(b, DIMGPU_E_INVALID_ARG, "dimgpu_batch_reserve: only on a new, empty batch");
+    if (max_cells < 1 || max_instances < 1 || max_steps < 1)
+        return bfail(b, DIMGPU_E_INVALID_ARG, "dimgpu_batch_reserve: capacities must be positive");
+    const int V = 2 * b->nmat + b->dim;
+    const long long C = max_instances;
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < 2 && e == cudaSuccess; ++k)
+        e = cudaMalloc(&b->st_arena[k], sizeof(double) * (size_t)V * (size_t)max_cells);
+    if (e == cudaSuccess) e = cudaMalloc(&b->dt_arena, sizeof(double) * (size_t)max_steps);
+    if (e == cudaSuccess)
+        e = cudaMalloc(&b->scratch, sizeof(double) * (size_t)staged_scratch_doubles(b->nmat, b->dim) *
+                                        (size_t)max_cells);
+    // every instance's work blocks round up to 256 cells: at most one extra block each
+    const long long nblocks = (max_cells + 255) / 256 + C;
+    if (e == cudaSuccess) e = cudaMalloc(&b->blockmin, sizeof(double) * (size_t)nblocks);
+    if (e == cudaSuccess) e = cudaMalloc(&b->tab, sizeof(BInst) * (size_t)C);
+    if (e == cudaSuccess) e = cudaMalloc(&b->cell_prefix, sizeof(long long) * (size_t)(C + 1));
+    if (e == cudaSuccess) e = cudaMalloc(&b->bc_prefix, sizeof(long long) * (size_t)(C + 1));
+    if (e == cudaSuccess) e = cudaMallocHost(&b->tab_pinned, sizeof(BInst) * (size_t)C);
+    if (e == cudaSuccess) e = cudaMallocHost(&b->prefix_pinned, sizeof(long long) * 2 * (size_t)(C + 1));
+    if (e != cudaSuccess) {
+        for (auto& p : b->st_arena) { cudaFree(p); p = nullptr; }
+        cudaFree(b->dt_arena); cudaFree(b->scratch); cudaFree(b->blockmin); cudaFree(b->tab);
+        cudaFree(b->cell_prefix); cudaFree(b->bc_prefix);
+        cudaFreeHost(b->tab_pinned); cudaFreeHost(b->prefix_pinned);
+        b->dt_arena = b->scratch = b->blockmin = nullptr;
+        b->tab = nullptr;
+        b->cell_prefix = b->bc_prefix = b->prefix_pinned = nullptr;
+        b->tab_pinned = nullptr;
+        return bcuda(b, e, "dimgpu_batch_reserve");
+    }
+    b->scratch_cap = (long long)staged_scratch_doubles(b->nmat, b->dim) * max_cells;
+    b->blockmin_cap = nblocks;
+    b->tab_cap = C;
+    b->arena = true;
+    b->cells.reset(max_cells);
+    b->dts.reset(max_steps);
+    drop_graphs(b);
+    b->dirty = true;
+    return DIMGPU_OK;
+}
+
 int dimgpu_batch_destroy(dimgpu_batch* b)
 {
     if (!b) return DIMGPU_OK;
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
-    for (auto& h : b->inst) {
-        cudaFree(h.dev.st[0]);
-        cudaFree(h.dev.st[1]);
-        cudaFree(h.dev.dtlog);
-    }
+    if (!b->arena)
+        for (auto& h : b->inst) free_instance(b, h);
+    for (auto& p : b->st_arena) cudaFree(p);
+    cudaFree(b->dt_arena);
+    cudaFreeHost(b->tab_pinned);
+    cudaFreeHost(b->prefix_pinned);
     cudaFree(b->tab);
     cudaFree(b->cell_prefix);
     cudaFree(b->bc_prefix);
@@ -305,9 +454,9 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
         if (!(d->mat[k].gamma > 1.0)) return bfail(b, DIMGPU_E_INVALID_ARG, "gamma must be > 1");
     }
     if (d->lambda_model < 0 || d->lambda_model > 2) return bfail(b, DIMGPU_E_INVALID_ARG, "unknown lambda model");
+    if (b->arena && (long long)b->inst.size() >= b->tab_cap)
+        return bfail(b, DIMGPU_E_OOM, "dimgpu_batch_add: the reserved instance table is full");
 
-    cudaError_t e = pull_counters(b);
-    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_add");
     HostInst h{};
     h.id = b->next_id++;
     h.desc = *d;
@@ -315,6 +464,7 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
     h.nbc = boundary_cells(*d);
     h.steps_total = steps;
     h.steps_left = steps;
+    h.cell_off = h.dt_off = -1;
     std::memset(&h.dev, 0, sizeof h.dev);
     BInst& I = h.dev;
     int kind[kMaxMat];
@@ -339,16 +489,32 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
     I.mixed = d->precision == DIMGPU_PRECISION_MIXED ? 1 : 0;
     I.cfl = cfl;
     I.dt_max = dt_max;
-    const size_t bytes = sizeof(double) * (size_t)(2 * d->nmat + d->dim) * (size_t)ncell;
-    e = cudaMalloc(&I.st[0], bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&I.st[1], bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&I.dtlog, sizeof(double) * (size_t)std::max(steps, 1));
-    if (e == cudaSuccess) e = cudaMemcpyAsync(I.st[b->parity], soa, bytes, cudaMemcpyHostToDevice, b->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    const int V = 2 * d->nmat + d->dim;
+    const size_t bytes = sizeof(double) * (size_t)V * (size_t)ncell;
+    cudaError_t e = cudaSuccess;
+    if (b->arena) {
+        // no allocation, no synchronisation: ranges of the reserved arenas
+        h.cell_off = b->cells.alloc(ncell);
+        if (h.cell_off < 0) return bfail(b, DIMGPU_E_OOM, "dimgpu_batch_add: no room for the grid in the reserved cells");
+        h.dt_off = b->dts.alloc(std::max(steps, 1));
+        if (h.dt_off < 0) {
+            b->cells.release(h.cell_off, ncell);
+            return bfail(b, DIMGPU_E_OOM, "dimgpu_batch_add: no room for the steps in the reserved dt log");
+        }
+        I.st[0] = b->st_arena[0] + (size_t)V * (size_t)h.cell_off;
+        I.st[1] = b->st_arena[1] + (size_t)V * (size_t)h.cell_off;
+        I.dtlog = b->dt_arena + h.dt_off;
+        e = cudaMemcpyAsync(I.st[0], soa, bytes, cudaMemcpyHostToDevice, b->stream);
+    }
+    else {
+        e = cudaMalloc(&I.st[0], bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&I.st[1], bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&I.dtlog, sizeof(double) * (size_t)std::max(steps, 1));
+        if (e == cudaSuccess) e = cudaMemcpyAsync(I.st[0], soa, bytes, cudaMemcpyHostToDevice, b->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+    }
     if (e != cudaSuccess) {
-        cudaFree(I.st[0]);
-        cudaFree(I.st[1]);
-        cudaFree(I.dtlog);
+        free_instance(b, h);
         return bcuda(b, e, "dimgpu_batch_add");
     }
     b->inst.push_back(h);
@@ -360,14 +526,12 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
 int dimgpu_batch_remove(dimgpu_batch* b, int id)
 {
     if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
-    cudaError_t e = pull_counters(b);
-    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_remove");
     for (size_t i = 0; i < b->inst.size(); ++i) {
         if (b->inst[i].id != id) continue;
-        cudaStreamSynchronize(b->stream);
-        cudaFree(b->inst[i].dev.st[0]);
-        cudaFree(b->inst[i].dev.st[1]);
-        cudaFree(b->inst[i].dev.dtlog);
+        // Arena mode: the range is reused only by later work on the same
+        // stream, which runs after every step already enqueued.
+        if (!b->arena) cudaStreamSynchronize(b->stream);
+        free_instance(b, b->inst[i]);
         b->inst.erase(b->inst.begin() + (long)i);
         b->dirty = true;
         return DIMGPU_OK;
@@ -375,57 +539,61 @@ int dimgpu_batch_remove(dimgpu_batch* b, int id)
     return bfail(b, DIMGPU_E_INVALID_ARG, "no instance with this id");
 }
 
-// Advance every instance with steps left by up to n steps.
-int dimgpu_batch_run(dimgpu_batch* b, int n)
+// Enqueue up to n steps of every instance with steps left, without waiting.
+int dimgpu_batch_enqueue(dimgpu_batch* b, int n)
 {
     if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
     if (n < 0) return bfail(b, DIMGPU_E_INVALID_ARG, "negative step count");
     if (b->inst.empty() || n == 0) return DIMGPU_OK;
     cudaError_t e = cudaSuccess;
     if (b->dirty) {
-        e = pull_counters(b);
-        if (e == cudaSuccess) e = rebuild(b);
-        if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
+        e = rebuild(b);
+        if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_enqueue");
     }
     const BatchLaunch L = launch_args(b);
-    const bool odd = (b->dim % 2) == 1;
     int done = 0;
     while (done < n && e == cudaSuccess) {
         if (n - done >= kGraphSteps) {
-            cudaGraphExec_t& g = b->graph[b->parity];
-            if (!g) {
+            if (!b->graph) {
                 cudaGraph_t graph;
                 e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
-                int par = b->parity;
-                for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) {
-                    e = one_step(b, L, par);
-                    if (odd) par = 1 - par;
-                }
+                for (int k = 0; k < kGraphSteps && e == cudaSuccess; ++k) e = one_step(b, L);
                 cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
                 if (e == cudaSuccess) e = e2;
                 if (e == cudaSuccess) {
-                    e = cudaGraphInstantiate(&g, graph, 0);
+                    e = cudaGraphInstantiate(&b->graph, graph, 0);
                     cudaGraphDestroy(graph);
                 }
                 if (e != cudaSuccess) break;
             }
-            e = cudaGraphLaunch(g, b->stream);
+            e = cudaGraphLaunch(b->graph, b->stream);
             count_launches((long long)kGraphSteps * (2 + 6 * b->dim));  // batch_step: cfl, finalize, 6 per axis
-            done += kGraphSteps;  // kGraphSteps is even: the parity is unchanged
+            done += kGraphSteps;
         }
         else {
-            e = one_step(b, L, b->parity);
+            e = one_step(b, L);
             count_launches(2 + 6 * b->dim);
-            if (odd) b->parity = 1 - b->parity;
             done += 1;
         }
     }
-    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
-    for (auto& h : b->inst) h.steps_left = std::max(0, h.steps_left - n);
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_enqueue");
+    // host mirror: an instance with L steps left ran min(n, L) of them, and
+    // ran in the last one iff L >= n
+    for (auto& h : b->inst) {
+        h.dev.run = h.steps_left >= n ? 1 : 0;
+        h.steps_left = std::max(0, h.steps_left - n);
+    }
+    return DIMGPU_OK;
+}
+
+// Wait for every enqueued step; report a non-finite state or time step.
+int dimgpu_batch_wait(dimgpu_batch* b)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
     int flag = 0;
-    e = cudaMemcpyAsync(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
+    cudaError_t e = cudaMemcpyAsync(&flag, b->err, sizeof(int), cudaMemcpyDeviceToHost, b->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
-    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_run");
+    if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_wait");
     if (flag) {
         cudaMemsetAsync(b->err, 0, sizeof(int), b->stream);
         if (flag & kErrNonFinite)
@@ -433,6 +601,14 @@ int dimgpu_batch_run(dimgpu_batch* b, int n)
         return bfail(b, DIMGPU_E_NONFINITE, "run_dim_case: non-positive timestep");
     }
     return DIMGPU_OK;
+}
+
+// Advance every instance with steps left by up to n steps and wait.
+int dimgpu_batch_run(dimgpu_batch* b, int n)
+{
+    const int rc = dimgpu_batch_enqueue(b, n);
+    if (rc != DIMGPU_OK) return rc;
+    return dimgpu_batch_wait(b);
 }
 
 // Steps run and left for one instance (host-side mirror, no device sync).
@@ -459,7 +635,8 @@ int dimgpu_batch_download(dimgpu_batch* b, int id, double* soa, size_t count, do
         if (soa && count != want) return bfail(b, DIMGPU_E_INVALID_ARG, "dimgpu_batch_download: size mismatch");
         cudaError_t e = cudaSuccess;
         if (soa)
-            e = cudaMemcpyAsync(soa, h.dev.st[b->parity], sizeof(double) * want, cudaMemcpyDeviceToHost, b->stream);
+            e = cudaMemcpyAsync(soa, h.dev.st[current_buffer(b, h)], sizeof(double) * want, cudaMemcpyDeviceToHost,
+                                b->stream);
         const int ndone = h.steps_total - h.steps_left;
         if (e == cudaSuccess && dts && ndone > 0)
             e = cudaMemcpyAsync(dts, h.dev.dtlog, sizeof(double) * (size_t)ndone, cudaMemcpyDeviceToHost, b->stream);
@@ -483,6 +660,15 @@ int dimgpu_batch_set_grid(dimgpu_batch* b, int ctas)
 }
 
 int dimgpu_batch_size(const dimgpu_batch* b) { return b ? (int)b->inst.size() : 0; }
+
+// Cells and dt-log entries in use in the reserved arenas (0 outside arena mode).
+int dimgpu_batch_arena_used(const dimgpu_batch* b, long long* cells, long long* dt_entries)
+{
+    if (!b) return bfail(nullptr, DIMGPU_E_INVALID_ARG, "null batch");
+    if (cells) *cells = b->arena ? b->cells.used() : 0;
+    if (dt_entries) *dt_entries = b->arena ? b->dts.used() : 0;
+    return DIMGPU_OK;
+}
 
 // Run on a caller-owned stream (NULL: the batch's own).  Captured graphs are
 // kept: replaying them on another stream is valid.

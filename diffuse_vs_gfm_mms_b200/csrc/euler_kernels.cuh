@@ -102,7 +102,7 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // of that latency than the few spilled registers (L1-resident) cost.
 template<int D, int DIR>
 __global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
-                                                             Grid g, Mats M, int T, int W, int ntile, int ngx,
+                                                             __grid_constant__ const Grid g, __grid_constant__ const Mats M, int T, int W, int ntile, int ngx,
                                                              const double* __restrict__ dtp, int* __restrict__ err,
                                                              int ends_copy)
 {
@@ -246,7 +246,7 @@ __global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __res
 // CFL partial minima (compute_dt_cfl_materials[_unsplit],
 // src/sim/solver/cfl.hpp:64-187), finished by the DIM finalize kernel.
 template<int D>
-__global__ void __launch_bounds__(256) euler_cfl_kernel(const double* __restrict__ st, Grid g, Mats M, double cfl,
+__global__ void __launch_bounds__(256) euler_cfl_kernel(const double* __restrict__ st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, double cfl,
                                                         int unsplit, double* __restrict__ blockmin,
                                                         int* __restrict__ err)
 {
@@ -370,7 +370,7 @@ __device__ void euler_bc_cell(const Grid& g, const Mats& M, double* st, const in
 // Boundary shell as planes (as bc_kernel): plane 2a+side holds the cells
 // with idx[a] at that side whose lower axes are interior.
 template<int D>
-__global__ void __launch_bounds__(256) euler_bc_kernel(double* st, Grid g, Mats M, long long plane0,
+__global__ void __launch_bounds__(256) euler_bc_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, long long plane0,
                                                        long long plane1, long long plane2)
 {
     const long long count[3] = {plane0, plane1, plane2};
@@ -397,7 +397,7 @@ __global__ void __launch_bounds__(256) euler_bc_kernel(double* st, Grid g, Mats 
 }
 
 template<int D>
-__global__ void euler_bc_serial_kernel(double* st, Grid g, Mats M)
+__global__ void euler_bc_serial_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M)
 {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     for (long long linear = 0; linear < g.ncell; ++linear) {
@@ -417,7 +417,7 @@ __global__ void euler_bc_serial_kernel(double* st, Grid g, Mats M)
 template<int D>
 __global__ void __launch_bounds__(256) euler_accumulate_kernel(double* __restrict__ acc,
                                                                const double* __restrict__ dir_state,
-                                                               const double* __restrict__ base, Grid g, Mats M,
+                                                               const double* __restrict__ base, __grid_constant__ const Grid g, __grid_constant__ const Mats M,
                                                                int enforce)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;

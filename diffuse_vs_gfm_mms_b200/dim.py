@@ -15,6 +15,7 @@ reference's time loop in src/app/solver/run_dim.hpp:88-154 needs);
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -37,6 +38,24 @@ class StepResult:
 def _times_dict(t: PhaseTimes) -> dict:
     return {"cfl_seconds": t.cfl_ms * 1e-3, "sweep_seconds": t.sweep_ms * 1e-3,
             "boundary_seconds": t.boundary_ms * 1e-3}
+
+
+class CsvWriter:
+    """An asynchronous CSV snapshot (dimgpu_csv_write_async)."""
+
+    def __init__(self, handle):
+        self._h = handle
+
+    def wait(self) -> None:
+        if self._h:
+            h, self._h = self._h, None
+            check(lib().dimgpu_csv_wait(h))
+
+    def __del__(self):
+        try:
+            self.wait()
+        except Exception:
+            pass
 
 
 class Session:
@@ -139,6 +158,37 @@ class Session:
         out = np.zeros(self.desc.nmat + self.desc.dim + 2)
         self._check(lib().dimgpu_boundary_flux(self._h, dptr(out)))
         return out
+
+    # ---- initial fields on the device, CSV snapshots
+    def init_shock_bubble(self, ic: dict) -> None:
+        """Write the shock-bubble field (workloads.shock_bubble_2d_setup's
+        parameters) into the device state: the same bits as the host
+        generator workloads.shock_bubble_2d."""
+        st = abi.fill_struct(abi.ShockBubbleIC(), ic)
+        self._check(lib().dimgpu_init_shock_bubble(self._h, C.byref(st)))
+
+    def init_bubble_cloud(self, ic: dict, bubbles) -> None:
+        """Write the bubble-cloud field (workloads.bubble_cloud_3d_setup's
+        parameters and bubbles) into the device state: the same bits as the
+        host generator workloads.bubble_cloud_3d."""
+        st = abi.fill_struct(abi.BubbleCloudIC(), ic)
+        arr = (abi.BubbleIC * max(1, len(bubbles)))()
+        for b, (c, r, lo, hi) in enumerate(bubbles):
+            abi.fill_struct(arr[b], {"center": c, "radius": r, "box_lo": lo, "box_hi": hi})
+        self._check(lib().dimgpu_init_bubble_cloud(self._h, C.byref(st), arr, len(bubbles)))
+
+    def write_csv_async(self, filename: str, domain_min, domain_max, threads: int = 0) -> "CsvWriter":
+        """Start writing the current state as dim::write_csv does
+        (src/io/dim_write_csv.hpp:15-125); the session may keep stepping.
+        Call .wait() on the result."""
+        lo = np.zeros(3)
+        hi = np.zeros(3)
+        lo[:len(domain_min)] = domain_min
+        hi[:len(domain_max)] = domain_max
+        h = C.c_void_p()
+        self._check(lib().dimgpu_csv_write_async(self._h, os.fsencode(filename), dptr(lo), dptr(hi), threads,
+                                                 C.byref(h)))
+        return CsvWriter(h)
 
     # ---- tuning and measurement
     def set_stream(self, stream_handle: int | None) -> None:

@@ -52,6 +52,24 @@ SIGNATURES = {
     "dimgpu_batch_set_stream": ([C.c_void_p, C.c_void_p], C.c_int),
     "dimgpu_advance_one_step": ([_D, _DP, _DP, C.c_double, C.c_double, _DP,
                                  C.POINTER(abi.PhaseTimes)], C.c_int),
+    "dimgpu_batch_reserve": ([C.c_void_p, C.c_longlong, C.c_int, C.c_longlong], C.c_int),
+    "dimgpu_batch_arena_used": ([C.c_void_p, C.POINTER(C.c_longlong), C.POINTER(C.c_longlong)], C.c_int),
+    "dimgpu_batch_enqueue": ([C.c_void_p, C.c_int], C.c_int),
+    "dimgpu_batch_wait": ([C.c_void_p], C.c_int),
+    "dimgpu_init_shock_bubble": ([_S, C.POINTER(abi.ShockBubbleIC)], C.c_int),
+    "dimgpu_init_bubble_cloud": ([_S, C.POINTER(abi.BubbleCloudIC), C.POINTER(abi.BubbleIC), C.c_int], C.c_int),
+    "dimgpu_csv_write_async": ([_S, C.c_char_p, _DP, _DP, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
+    "dimgpu_csv_wait": ([C.c_void_p], C.c_int),
+    "dimgpu_server_create": ([C.POINTER(abi.ServerConfig), C.POINTER(C.c_void_p)], C.c_int),
+    "dimgpu_server_destroy": ([C.c_void_p], C.c_int),
+    "dimgpu_server_last_error": ([C.c_void_p], C.c_char_p),
+    "dimgpu_server_submit": ([C.c_void_p, _D, _DP, C.c_int, C.c_double, C.c_double, C.POINTER(C.c_longlong)],
+                             C.c_int),
+    "dimgpu_server_poll": ([C.c_void_p, C.c_longlong, C.POINTER(C.c_int), _DP, C.c_size_t, _DP,
+                           C.POINTER(C.c_double)], C.c_int),
+    "dimgpu_server_cancel": ([C.c_void_p, C.c_longlong], C.c_int),
+    "dimgpu_server_drain": ([C.c_void_p], C.c_int),
+    "dimgpu_server_stats": ([C.c_void_p, C.POINTER(abi.ServerCounters)], C.c_int),
 }
 
 _lib = None

@@ -1,28 +1,32 @@
 """Continuous-batching serving loop for DIM solve requests.
 
 Requests (a grid, its initial state and a step budget) arrive over time.  The
-server admits them first-come-first-served as long as their device
-footprint fits the HBM budget and a slot is free, keeps every admitted
-solve's state resident on the GPU, and advances all admitted solves together
-in quanta of a few steps through the batched form (one ``Batch`` per material
-count and dimension).  A request that arrives while others run joins at the
-next quantum; a finished request is downloaded and its memory returned at
-once, which is what lets the queue drain into the freed room.
+server (dimgpu_server_* in libdimgpu.so, a native server thread) admits them
+first-come-first-served as long as their device footprint fits the HBM
+budget and a slot is free, keeps every admitted solve's state resident on the
+GPU in device memory reserved once (admission allocates and synchronises
+nothing), and advances all admitted solves together in quanta of a few steps
+through the batched form, one batch per material count and dimension, each
+on its own stream so that they overlap.  A request that arrives while others
+run joins at the next quantum; a finished request is downloaded and its
+memory returned at once, which is what lets the queue drain into the freed
+room.
 
 Every solve's arithmetic is the single-grid step's, so a result does not
 depend on what else was in flight (tests/test_gpu_serving.py).
 """
 from __future__ import annotations
 
+import ctypes as C
 import math
 import time
-from collections import deque
 from dataclasses import dataclass, field
 
 import numpy as np
 
-from .abi import PRECISION_MIXED, Desc
-from .batch import Batch
+from . import abi
+from .abi import PRECISION_MIXED, Desc, dptr
+from .native import DimGpuError, lib
 
 # Device doubles per cell: two state copies plus the staged-sweep scratch
 # (csrc/dimgpu_api.cu staged_scratch_doubles).
@@ -80,24 +84,36 @@ class ServerStats:
 
 
 class Server:
-    """Admission, resident state and batched stepping of DIM solves."""
+    """The continuous-batching server (dimgpu_server_* in libdimgpu.so): a
+    native server thread admits, steps and retires solves; this class submits
+    requests at their arrival times and collects the results."""
 
     def __init__(self, hbm_budget_bytes: float = 150e9, max_slots: int = 128, quantum: int = 8,
-                 stream_handle: int | None = None):
+                 dim_share=(0.4, 0.6, 0.0), max_steps_per_solve: int = 4096):
+        cfg = abi.ServerConfig()
+        cfg.hbm_budget_bytes = float(hbm_budget_bytes)
+        for k in range(3):
+            cfg.dim_share[k] = float(dim_share[k])
+        cfg.max_slots = max_slots
+        cfg.quantum = quantum
+        cfg.max_steps_per_solve = max_steps_per_solve
+        h = C.c_void_p()
+        self._check(lib().dimgpu_server_create(C.byref(cfg), C.byref(h)), None)
+        self._h = h
         self.budget = float(hbm_budget_bytes)
-        self.max_slots = max_slots
-        self.quantum = quantum
-        self.stream = stream_handle
-        self.batches: dict[tuple[int, int], Batch] = {}
-        self.pending: deque[Request] = deque()
-        self.active: dict[int, tuple[Request, int, float]] = {}  # rid -> (request, instance id, admitted)
-        self.used = 0
-        self.cancelled: set[int] = set()
+        self.ids: dict[int, int] = {}        # request rid -> server request id
+        self.reqs: dict[int, Request] = {}
+
+    def _check(self, rc: int, h=...) -> None:
+        if rc != 0:
+            handle = self._h if h is ... else h
+            msg = lib().dimgpu_server_last_error(handle) if handle else lib().dimgpu_last_error(None)
+            raise DimGpuError(rc, msg.decode() if msg else "")
 
     def close(self):
-        for b in self.batches.values():
-            b.close()
-        self.batches.clear()
+        if getattr(self, "_h", None):
+            lib().dimgpu_server_destroy(self._h)
+            self._h = None
 
     def __enter__(self):
         return self
@@ -105,87 +121,86 @@ class Server:
     def __exit__(self, *exc):
         self.close()
 
-    def _batch(self, desc: Desc) -> Batch:
-        key = (desc.nmat, desc.dim)
-        if key not in self.batches:
-            b = Batch(*key)
-            if self.stream:
-                b.set_stream(self.stream)
-            self.batches[key] = b
-        return self.batches[key]
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def submit(self, req: Request) -> None:
-        if footprint_bytes(req.desc, req.steps) > self.budget:
-            raise ValueError(f"request {req.rid} needs more device memory than the whole budget")
-        self.pending.append(req)
+        U = np.ascontiguousarray(req.U, dtype=np.float64)
+        nid = C.c_longlong()
+        self._check(lib().dimgpu_server_submit(self._h, C.byref(req.desc), dptr(U), req.steps, req.cfl, req.dt_max,
+                                               C.byref(nid)))
+        self.ids[req.rid] = nid.value
+        self.reqs[req.rid] = req
+
+    def state(self, rid: int) -> int:
+        st = C.c_int()
+        self._check(lib().dimgpu_server_poll(self._h, self.ids[rid], C.byref(st), None, 0, None, None))
+        return st.value
 
     def cancel(self, rid: int) -> bool:
-        """Drop a queued or running request; True if it was found."""
-        for r in list(self.pending):
-            if r.rid == rid:
-                self.pending.remove(r)
-                return True
-        if rid in self.active:
-            req, iid, _ = self.active.pop(rid)
-            self._batch(req.desc).remove(iid)
-            self.used -= footprint_bytes(req.desc, req.steps)
-            self.cancelled.add(rid)
-            return True
-        return False
+        """Drop a queued or running request; True if it was still known."""
+        if rid not in self.ids:
+            return False
+        return lib().dimgpu_server_cancel(self._h, self.ids[rid]) == 0
 
-    def _admit(self, now: float) -> None:
-        while self.pending and len(self.active) < self.max_slots:
-            req = self.pending[0]
-            need = footprint_bytes(req.desc, req.steps)
-            if self.used + need > self.budget:
-                break
-            self.pending.popleft()
-            iid = self._batch(req.desc).add(req.desc, req.U, req.steps, req.cfl, req.dt_max)
-            self.active[req.rid] = (req, iid, now)
-            self.used += need
+    def collect(self, rid: int):
+        """(state, U, dts, latency) of a request; U / dts are meaningful only
+        when it is done (the request is then forgotten by the server)."""
+        req = self.reqs[rid]
+        st, lat = C.c_int(), C.c_double()
+        U = np.empty((req.desc.nvar, req.desc.ncell))
+        dts = np.zeros(max(req.steps, 1))
+        self._check(lib().dimgpu_server_poll(self._h, self.ids[rid], C.byref(st), dptr(U), U.size, dptr(dts),
+                                             C.byref(lat)))
+        if st.value in (abi.REQ_DONE, abi.REQ_CANCELLED):
+            del self.ids[rid]
+        return st.value, U, dts[:req.steps], lat.value
 
-    def _retire(self, now_fn) -> list[Result]:
-        out = []
-        for rid in list(self.active):
-            req, iid, admitted = self.active[rid]
-            b = self._batch(req.desc)
-            done, left = b.status(iid)
-            if left > 0:
-                continue
-            U, dts = b.download(iid)
-            b.remove(iid)
-            self.used -= footprint_bytes(req.desc, req.steps)
-            del self.active[rid]
-            out.append(Result(rid, U, dts, req.arrival, admitted, now_fn()))
+    def drain(self) -> None:
+        self._check(lib().dimgpu_server_drain(self._h))
+
+    def counters(self) -> abi.ServerCounters:
+        out = abi.ServerCounters()
+        self._check(lib().dimgpu_server_stats(self._h, C.byref(out)))
         return out
 
     def serve(self, requests: list[Request], clock=time.perf_counter) -> ServerStats:
-        """Run the event loop until every request has finished.  Arrivals
-        follow each request's `arrival` offset in wall-clock time."""
+        """Submit every request at its `arrival` offset (wall clock) and
+        collect the results as they finish."""
         stats = ServerStats()
         reqs = sorted(requests, key=lambda r: r.arrival)
         t0 = clock()
         now_fn = lambda: clock() - t0  # noqa: E731
+        submit_at: dict[int, float] = {}
+        outstanding: list[int] = []
         i = 0
-        total = len(reqs)
-        while len(stats.results) + len(self.cancelled) < total:
+        while i < len(reqs) or outstanding:
             now = now_fn()
-            while i < total and reqs[i].arrival <= now:
+            while i < len(reqs) and reqs[i].arrival <= now:
                 self.submit(reqs[i])
+                submit_at[reqs[i].rid] = now_fn()
+                outstanding.append(reqs[i].rid)
                 i += 1
-            self._admit(now)
-            stats.peak_bytes = max(stats.peak_bytes, self.used)
-            stats.peak_slots = max(stats.peak_slots, len(self.active))
-            if not self.active:
-                if i < total:
-                    time.sleep(max(0.0, min(0.002, reqs[i].arrival - now_fn())))
-                continue
-            for b in self.batches.values():
-                if len(b):
-                    b.run(self.quantum)
-            stats.quanta += 1
-            stats.results.extend(self._retire(now_fn))
+            still = []
+            for rid in outstanding:
+                if self.state(rid) != abi.REQ_DONE:
+                    still.append(rid)
+                    continue
+                _, U, dts, lat = self.collect(rid)
+                r = self.reqs[rid]
+                stats.results.append(Result(rid, U, dts, r.arrival, submit_at[rid], submit_at[rid] + lat))
+            outstanding = still
+            if outstanding or i < len(reqs):
+                nxt = reqs[i].arrival - now_fn() if i < len(reqs) else 0.002
+                time.sleep(max(0.0, min(0.002, nxt)))
         stats.elapsed = now_fn()
+        c = self.counters()
+        stats.peak_bytes = int(c.peak_bytes)
+        stats.peak_slots = int(c.peak_resident)
+        stats.quanta = int(c.quanta)
         return stats
 
 

@@ -48,9 +48,45 @@ def prim_to_cons_np(dim: int, mats, alpha: np.ndarray, rho: np.ndarray,
     return out
 
 
+# ---- portable exp / tanh --------------------------------------------------------
+#
+# The initial fields are also generated on the device (csrc/dim_io.cuh), and
+# both generators must give the same bits.  Library exp / tanh differ between
+# numpy, libm and CUDA in the last bits, so the indicator uses its own exp
+# from IEEE +, -, *, / and exact scaling only (Cody-Waite reduction with
+# fdlibm's split of ln 2, then a degree-13 Taylor polynomial in Horner form,
+# error below 1e-16 relative), evaluated in the same order on both sides.
+LN2_HI = 6.93147180369123816490e-01
+LN2_LO = 1.90821492927058770002e-10
+INV_LN2 = 1.44269504088896338700e+00
+EXP_COEF = [1.0 / math.factorial(n) for n in range(14)]   # 1/0! .. 1/13!
+
+
+def portable_exp(x):
+    """exp(x) for |x| <= 700 with the device generator's arithmetic."""
+    x = np.asarray(x, dtype=np.float64)
+    k = np.floor(x * INV_LN2 + 0.5)
+    r = (x - k * LN2_HI) - k * LN2_LO
+    p = np.full_like(r, EXP_COEF[13])
+    for n in range(12, -1, -1):
+        p = p * r + EXP_COEF[n]
+    return np.ldexp(p, k.astype(np.int64))
+
+
+def portable_tanh(y):
+    """tanh(y) = (e - 1) / (e + 1) with e = exp(2|y|), odd; 1 beyond |y| = 20."""
+    y = np.asarray(y, dtype=np.float64)
+    a = np.minimum(np.abs(y), 20.0)
+    e = portable_exp(2.0 * a)
+    t = (e - 1.0) / (e + 1.0)
+    t = np.where(np.abs(y) > 20.0, 1.0, t)
+    return np.where(y < 0.0, -t, t)
+
+
 def smooth_indicator(signed_distance, thickness, sharpness=2.0):
-    """Reference tanh indicator, 1 inside (s <= 0), 0 outside."""
-    return 0.5 * (1.0 - np.tanh(max(sharpness, 1e-12) * signed_distance / thickness))
+    """Reference tanh indicator (src/setup/dim_initial_conditions.hpp:224-236),
+    1 inside (s <= 0), 0 outside, with the portable tanh."""
+    return 0.5 * (1.0 - portable_tanh(max(sharpness, 1e-12) * signed_distance / thickness))
 
 
 def _kind(p_inf: float) -> str:
@@ -118,48 +154,60 @@ def rankine_hugoniot(mach: float, gamma: float, rho1: float, p1: float):
     return rho2, u2, p2
 
 
-def shock_bubble_2d(N=(1024, 512), seed: int = 0) -> tuple[Desc, np.ndarray]:
-    """Config 1: Mach 1.22 shock at x = 0.6 hitting a light bubble.
-
-    Domain [0,2]x[0,1]; ambient gamma 1.4, rho 1, p 1; bubble gamma 1.67,
-    rho 0.138, radius 0.25 at (1, 0.5); post-shock slab x < 0.6 moving +x.
-    Transmissive in x, reflective in y.  (The seed is unused: the case is
-    deterministic.)
-    """
+def shock_bubble_2d_setup(N=(1024, 512)):
+    """Descriptor and initial-field parameters of config 1 (the one definition
+    the host generator below and the device generator,
+    dimgpu_init_shock_bubble, both use)."""
     nx, ny = N
     dx = [2.0 / nx, 1.0 / ny]
     mats = [("ideal_gas", 1.4, 0.0), ("ideal_gas", 1.67, 0.0)]
     desc = make_desc(2, N, dx, mats, bc_lo=["transmissive", "reflective"],
                      bc_hi=["transmissive", "reflective"])
     rho2, u2, p2 = rankine_hugoniot(1.22, 1.4, 1.0, 1.0)
+    ic = dict(center=(1.0, 0.5), radius=0.25, thickness=2.0 * max(dx), sharpness=2.0, shock_x=0.6,
+              zero_below=1e-14, rho_post=rho2, u_post=u2, p_post=p2, rho_pre=1.0, p_pre=1.0,
+              rho_bubble=0.138, p_bubble=1.0)
+    return desc, ic
+
+
+def shock_bubble_2d(N=(1024, 512), seed: int = 0) -> tuple[Desc, np.ndarray]:
+    """Config 1: Mach 1.22 shock at x = 0.6 hitting a light bubble.
+
+    Domain [0,2]x[0,1]; ambient gamma 1.4, rho 1, p 1; bubble gamma 1.67,
+    rho 0.138, radius 0.25 at (1, 0.5); post-shock slab x < 0.6 moving +x.
+    Transmissive in x, reflective in y.  (The seed is unused: the case is
+    deterministic.)  dimgpu_init_shock_bubble builds the same bits on the
+    device.
+    """
+    desc, ic = shock_bubble_2d_setup(N)
+    nx, ny = N
+    dx = [desc.dx[0], desc.dx[1]]
+    mats = [(desc.mat[k].kind, desc.mat[k].gamma, desc.mat[k].p_inf) for k in range(2)]
     y, x = np.meshgrid((np.arange(ny) + 0.5) * dx[1], (np.arange(nx) + 0.5) * dx[0], indexing="ij")
     x = x.reshape(-1)
     y = y.reshape(-1)
-    sd = np.hypot(x - 1.0, y - 0.5) - 0.25
-    thick = 2.0 * max(dx)
-    ab = smooth_indicator(sd, thick)
-    ab = np.where(ab <= 1e-14, 0.0, ab)
-    post = x < 0.6
-    rho_amb = np.where(post, rho2, 1.0)
-    p_amb = np.where(post, p2, 1.0)
-    u_amb = np.where(post, u2, 0.0)
+    cx, cy = ic["center"]
+    sd = np.sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy)) - ic["radius"]
+    ab = smooth_indicator(sd, ic["thickness"], ic["sharpness"])
+    ab = np.where(ab <= ic["zero_below"], 0.0, ab)
+    post = x < ic["shock_x"]
+    rho_amb = np.where(post, ic["rho_post"], ic["rho_pre"])
+    p_amb = np.where(post, ic["p_post"], ic["p_pre"])
+    u_amb = np.where(post, ic["u_post"], 0.0)
     n = x.size
     alpha = np.stack([1.0 - ab, ab])
-    rho = np.stack([rho_amb, np.full(n, 0.138)])
+    rho = np.stack([rho_amb, np.full(n, ic["rho_bubble"])])
     vel = np.stack([(1.0 - ab) * u_amb, np.zeros(n)])
-    p = (1.0 - ab) * p_amb + ab * 1.0
+    p = (1.0 - ab) * p_amb + ab * ic["p_bubble"]
     soa = prim_to_cons_np(2, mats, alpha, rho, vel, p)
     return desc, np.ascontiguousarray(soa)
 
 
-def bubble_cloud_3d(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64,
-                    pulse_width: float = 0.05) -> tuple[Desc, np.ndarray]:
-    """Config 2: 64 seeded air bubbles in water, 1e9 Pa slab at x < 0.05.
-
-    Water: stiffened gas gamma 4.4, p_inf 6e8, rho 1000, p 1e5.  Air: ideal
-    gamma 1.4, rho 1.2, p 1e5.  Radii U[0.02, 0.06], rejection-sampled to be
-    non-overlapping (with one cell of clearance).  Transmissive everywhere.
-    """
+def bubble_cloud_3d_setup(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64, pulse_width: float = 0.05):
+    """Descriptor, field parameters and bubbles of config 2 (shared by the
+    host generator below and dimgpu_init_bubble_cloud).  Each bubble is
+    (centre, radius, box_lo, box_hi): its indicator is evaluated only in the
+    box of cells within 6 interface thicknesses of its surface."""
     rng = np.random.default_rng(seed)
     nx, ny, nz = N
     dx = [1.0 / nx, 1.0 / ny, 1.0 / nz]
@@ -175,22 +223,43 @@ def bubble_cloud_3d(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64,
         if all(np.linalg.norm(c - b[0]) > r + b[1] + 2 * max(dx) for b in bubbles):
             bubbles.append((c, r))
     thick = 2.0 * max(dx)
-    ncell = nx * ny * nz
-    air = np.zeros(ncell)
-    air3 = air.reshape(nz, ny, nx)
     reach = 6.0 * thick
+    out = []
     for c, r in bubbles:
         lo = [max(0, int((c[a] - r - reach) / dx[a])) for a in range(3)]
         hi = [min(N[a], int((c[a] + r + reach) / dx[a]) + 1) for a in range(3)]
+        out.append((tuple(float(v) for v in c), float(r), lo, hi))
+    ic = dict(thickness=thick, sharpness=2.0, zero_below=1e-14, pulse_width=pulse_width, rho_liquid=1000.0,
+              rho_gas=1.2, p_ambient=1e5, p_pulse=1e9)
+    return desc, ic, out
+
+
+def bubble_cloud_3d(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64,
+                    pulse_width: float = 0.05) -> tuple[Desc, np.ndarray]:
+    """Config 2: 64 seeded air bubbles in water, 1e9 Pa slab at x < 0.05.
+
+    Water: stiffened gas gamma 4.4, p_inf 6e8, rho 1000, p 1e5.  Air: ideal
+    gamma 1.4, rho 1.2, p 1e5.  Radii U[0.02, 0.06], rejection-sampled to be
+    non-overlapping (with one cell of clearance).  Transmissive everywhere.
+    dimgpu_init_bubble_cloud builds the same bits on the device.
+    """
+    desc, ic, bubbles = bubble_cloud_3d_setup(N, seed, nbubbles, pulse_width)
+    nx, ny, nz = N
+    dx = [desc.dx[0], desc.dx[1], desc.dx[2]]
+    mats = [(desc.mat[k].kind, desc.mat[k].gamma, desc.mat[k].p_inf) for k in range(2)]
+    ncell = nx * ny * nz
+    air = np.zeros(ncell)
+    air3 = air.reshape(nz, ny, nx)
+    for c, r, lo, hi in bubbles:
         zs = (np.arange(lo[2], hi[2]) + 0.5) * dx[2]
         ys = (np.arange(lo[1], hi[1]) + 0.5) * dx[1]
         xs = (np.arange(lo[0], hi[0]) + 0.5) * dx[0]
         Z, Y, X = np.meshgrid(zs, ys, xs, indexing="ij")
-        sd = np.sqrt((X - c[0]) ** 2 + (Y - c[1]) ** 2 + (Z - c[2]) ** 2) - r
-        ind = smooth_indicator(sd, thick)
+        sd = np.sqrt((X - c[0]) * (X - c[0]) + (Y - c[1]) * (Y - c[1]) + (Z - c[2]) * (Z - c[2])) - r
+        ind = smooth_indicator(sd, ic["thickness"], ic["sharpness"])
         sub = air3[lo[2]:hi[2], lo[1]:hi[1], lo[0]:hi[0]]
         np.maximum(sub, ind, out=sub)
-    air[air <= 1e-14] = 0.0
+    air[air <= ic["zero_below"]] = 0.0
     out = np.empty((2 * 2 + 3, ncell))
     chunk = nx * ny * 16
     xs_all = (np.arange(nx) + 0.5) * dx[0]
@@ -199,9 +268,9 @@ def bubble_cloud_3d(N=(512, 512, 512), seed: int = 0, nbubbles: int = 64,
         a1 = air[s:e]
         n = e - s
         x = np.tile(xs_all, n // nx)
-        p = np.where(x < pulse_width, 1e9, 1e5)
+        p = np.where(x < ic["pulse_width"], ic["p_pulse"], ic["p_ambient"])
         alpha = np.stack([1.0 - a1, a1])
-        rho = np.stack([np.full(n, 1000.0), np.full(n, 1.2)])
+        rho = np.stack([np.full(n, ic["rho_liquid"]), np.full(n, ic["rho_gas"])])
         vel = np.zeros((3, n))
         out[:, s:e] = prim_to_cons_np(3, mats, alpha, rho, vel, p)
     return desc, out
@@ -218,7 +287,7 @@ def single_bubble_2d(N, seed: int = 0) -> tuple[Desc, np.ndarray]:
     cx, cy = rng.uniform(0.3, 0.7, size=2)
     r = rng.uniform(0.1, 0.25)
     y, x = np.meshgrid((np.arange(ny) + 0.5) * dx[1], (np.arange(nx) + 0.5) * dx[0], indexing="ij")
-    sd = (np.hypot(x - cx, y - cy) - r).reshape(-1)
+    sd = (np.sqrt((x - cx) * (x - cx) + (y - cy) * (y - cy)) - r).reshape(-1)
     ab = smooth_indicator(sd, 2.0 * max(dx))
     ab = np.clip(ab, ALPHA_FLOOR, 1.0 - ALPHA_FLOOR)
     n = sd.size

@@ -318,6 +318,159 @@ int dimgpu_batch_size(const dimgpu_batch* b);
 /* Run the batch's work on a caller-owned CUDA stream (NULL: its own). */
 int dimgpu_batch_set_stream(dimgpu_batch* b, void* cuda_stream);
 
+/* Arena mode, for hosts that admit and retire solves continuously: reserve
+ * once, on a new batch, device memory for at most `max_cells` cells over all
+ * resident instances, `max_instances` instances and `max_steps` logged time
+ * steps.  Afterwards dimgpu_batch_add and _remove allocate, free and
+ * synchronise nothing (ranges of the reserved memory; the initial state is
+ * copied asynchronously on the batch's stream), a full arena returns
+ * DIMGPU_E_OOM, and the captured step graph stays valid across every join
+ * and leave. */
+int dimgpu_batch_reserve(dimgpu_batch* b, long long max_cells, int max_instances, long long max_steps);
+
+/* Cells and dt-log entries of the arena in use. */
+int dimgpu_batch_arena_used(const dimgpu_batch* b, long long* cells, long long* dt_entries);
+
+/* dimgpu_batch_run without the wait: enqueue up to n steps of every instance
+ * with steps left on the batch's stream and return.  dimgpu_batch_wait waits
+ * for them and reports a non-finite state or time step of any of them. */
+int dimgpu_batch_enqueue(dimgpu_batch* b, int n);
+int dimgpu_batch_wait(dimgpu_batch* b);
+
+/* ---- the serving loop ----------------------------------------------------
+ * Continuous batching of DIM solve requests.  No counterpart in the
+ * reference, which runs one case per process (run_dim_case,
+ * src/app/solver/run_dim.hpp:20-178).  Requests are submitted from any host
+ * thread and queue in arrival order; a server thread admits them first come
+ * first served (per material count and dimension) into batches whose device
+ * memory was reserved once from the budget (dimgpu_batch_reserve), so
+ * admission allocates and synchronises nothing; every quantum it advances
+ * all resident solves, each group on its own stream so the groups overlap
+ * on the device, and retires the finished ones, which frees their room for
+ * the queue.  A result is exactly the single-grid step's. */
+typedef struct dimgpu_server dimgpu_server;
+
+typedef struct dimgpu_server_config {
+    double hbm_budget_bytes;   /* device memory for resident solves (states + step scratch) */
+    double dim_share[3];       /* fraction of the budget for 1D, 2D and 3D solves (sum <= 1) */
+    int max_slots;             /* resident solves at most */
+    int quantum;               /* steps per scheduling round */
+    int max_steps_per_solve;   /* largest step budget a request may ask for */
+} dimgpu_server_config;
+
+enum {
+    DIMGPU_REQ_QUEUED = 0,
+    DIMGPU_REQ_RUNNING = 1,
+    DIMGPU_REQ_DONE = 2,
+    DIMGPU_REQ_CANCELLED = 3,
+    DIMGPU_REQ_FAILED = 4
+};
+
+typedef struct dimgpu_server_counters {
+    long long submitted, completed, cancelled, failed, quanta, queued;
+    int resident, peak_resident;
+    double peak_bytes;
+} dimgpu_server_counters;
+
+int dimgpu_server_create(const dimgpu_server_config* cfg, dimgpu_server** out);
+int dimgpu_server_destroy(dimgpu_server* s);
+const char* dimgpu_server_last_error(const dimgpu_server* s);
+
+/* Queue a solve: the state (V * ncell doubles) is copied, so the caller's
+ * buffer is free on return.  A solve larger than its dimension's share of
+ * the budget returns DIMGPU_E_OOM. */
+int dimgpu_server_submit(dimgpu_server* s, const dimgpu_desc* desc, const double* soa, int steps,
+                         double cfl, double dt_max, long long* request_id);
+
+/* State of a request (DIMGPU_REQ_*).  For a finished request, latency_s is
+ * the time from submission to completion; with soa_out (count = V * ncell)
+ * the result and, if dts_out is not NULL, the dt of every step are copied
+ * out and the request is collected (forgotten).  A failed request returns
+ * DIMGPU_E_NONFINITE with its message and is collected. */
+int dimgpu_server_poll(dimgpu_server* s, long long request_id, int* state, double* soa_out, size_t count,
+                       double* dts_out, double* latency_s);
+
+/* Drop a queued or resident request; its room is freed at the next round. */
+int dimgpu_server_cancel(dimgpu_server* s, long long request_id);
+
+/* Wait until no request is queued or resident. */
+int dimgpu_server_drain(dimgpu_server* s);
+
+int dimgpu_server_stats(dimgpu_server* s, dimgpu_server_counters* out);
+
+/* ---- initial fields generated on the device ------------------------------
+ * The reference builds its initial field on the host cell by cell
+ * (initialise_dim_from_config, src/setup/dim_initial_conditions.hpp:608-628)
+ * with the tanh indicator 0.5 (1 - tanh(a s / thickness)) (smooth_indicator,
+ * :224-236) across diffuse interfaces.  These entry points write the two
+ * benchmark fields straight into a session's device state, so a 512^3 field
+ * (7.5 GB) is never built on the host or copied.  The tanh is the library's
+ * own (IEEE +, -, *, / and exact scaling), and the host generator in
+ * diffuse_vs_gfm_mms_b200/workloads.py uses the same arithmetic: both give the
+ * same bits. */
+
+/* Shock-bubble (2D, two materials): material 1 in the disc of `radius`
+ * around `center`, smeared by the indicator with `thickness` and
+ * `sharpness`, its fraction set to 0 where the indicator is <= zero_below;
+ * material 0 elsewhere, at (rho_post, u_post along x, p_post) for cell
+ * centres x < shock_x and (rho_pre, at rest, p_pre) beyond.  Velocity and
+ * pressure are the fraction-weighted mixes; the bubble is at rest at
+ * (rho_bubble, p_bubble). */
+typedef struct dimgpu_ic_shock_bubble {
+    double center[2];
+    double radius;
+    double thickness;
+    double sharpness;
+    double shock_x;
+    double zero_below;
+    double rho_post, u_post, p_post;
+    double rho_pre, p_pre;
+    double rho_bubble, p_bubble;
+} dimgpu_ic_shock_bubble;
+
+int dimgpu_init_shock_bubble(dimgpu_session* s, const dimgpu_ic_shock_bubble* ic);
+
+/* Bubble cloud (3D, two materials): material 1 (gas, density rho_gas) in
+ * spheres; each sphere's indicator is evaluated in its box of cells
+ * [box_lo, box_hi) only, and a cell's gas fraction is the largest of them (0
+ * where <= zero_below); material 0 (liquid, rho_liquid) elsewhere; at rest,
+ * pressure p_pulse for cell centres x < pulse_width and p_ambient beyond. */
+typedef struct dimgpu_ic_bubble {
+    double center[3];
+    double radius;
+    int box_lo[3];
+    int box_hi[3];
+} dimgpu_ic_bubble;
+
+typedef struct dimgpu_ic_bubble_cloud {
+    double thickness;
+    double sharpness;
+    double zero_below;
+    double pulse_width;
+    double rho_liquid, rho_gas;
+    double p_ambient, p_pulse;
+} dimgpu_ic_bubble_cloud;
+
+int dimgpu_init_bubble_cloud(dimgpu_session* s, const dimgpu_ic_bubble_cloud* ic,
+                             const dimgpu_ic_bubble* bubbles, int nbubbles);
+
+/* ---- asynchronous CSV snapshot -------------------------------------------
+ * Writes the session's current state as dim::write_csv does
+ * (src/io/dim_write_csv.hpp:15-125): same header, one row per cell in linear
+ * order, values printed as std::ostream prints a double ("%.6g"), cell
+ * centres domain_min + (i + 0.5) (domain_max - domain_min) / N.  The call
+ * copies the state into a device snapshot (ordered after the session's
+ * pending work; the session's later work waits for the copy only) and
+ * returns; a host thread then streams the per-cell values from the device
+ * in chunks and formats them with `threads` threads (0: all cores) while the
+ * session keeps stepping.  dimgpu_csv_wait joins the writer, frees it and
+ * returns its status.  DIM model only. */
+typedef struct dimgpu_csv_writer dimgpu_csv_writer;
+
+int dimgpu_csv_write_async(dimgpu_session* s, const char* filename, const double* domain_min,
+                           const double* domain_max, int threads, dimgpu_csv_writer** out);
+int dimgpu_csv_wait(dimgpu_csv_writer* w);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1467,3 +1467,56 @@ int oracle_solve_line(const dimgpu_desc* d, int n, int dir, double dt, double dx
     free(lin); free(lout); free(w.p); free(w.s); free(w.f); free(w.fv); free(w.pf);
     return rc;
 }
+
+/* dim::write_csv, src/io/dim_write_csv.hpp:15-125: header, then one row per
+ * cell in linear order with the values std::ostream prints by default
+ * ("%.6g"): cell centre (compute_cell_center, geometry.hpp:75-87, with
+ * dx = (max - min) / N), total density, velocity, pressure, internal energy
+ * max(safe_div(E - kinetic, rho), 0), fractions, material densities, masses. */
+int oracle_write_csv(const dimgpu_desc* d, const double* soa, const double* domain_min,
+                     const double* domain_max, const char* filename)
+{
+    const int rc0 = validate(d);
+    if (rc0) return rc0;
+    ctx_t c;
+    make_ctx(d, &c);
+    FILE* f = fopen(filename, "wb");
+    if (!f) { set_err("dim::write_csv: failed to open file"); return DIMGPU_E_INVALID_ARG; }
+    double dx[3];
+    for (int a = 0; a < c.dim; ++a) dx[a] = (domain_max[a] - domain_min[a]) / (double)d->N[a];
+    for (int a = 0; a < c.dim; ++a) fprintf(f, "x%d,", a);
+    fprintf(f, "rho,");
+    for (int a = 0; a < c.dim; ++a) fprintf(f, "u%d,", a);
+    fprintf(f, "p,e");
+    for (int k = 0; k < c.nmat; ++k) fprintf(f, ",alpha%d", k);
+    for (int k = 0; k < c.nmat; ++k) fprintf(f, ",rho_mat%d", k);
+    for (int k = 0; k < c.nmat; ++k) fprintf(f, ",mass%d", k);
+    fprintf(f, "\n");
+    const size_t n = field_cells(d);
+    for (size_t i = 0; i < n; ++i) {
+        st_t U;
+        pr_t P;
+        load_cell(&c, soa, n, i, &U);
+        cons_to_prim(&c, &U, &P);
+        const double rho = total_density(&c, &U);
+        double v2 = 0.0;
+        for (int a = 0; a < c.dim; ++a) v2 += P.vel[a] * P.vel[a];
+        const double kinetic = 0.5 * rho * v2;
+        const double ie = MAXD(safe_div(U.E - kinetic, rho, 1e-10), 0.0);
+        size_t rem = i;
+        for (int a = 0; a < c.dim; ++a) {
+            const size_t idx = rem % (size_t)d->N[a];
+            rem /= (size_t)d->N[a];
+            fprintf(f, "%.6g,", domain_min[a] + ((double)idx + 0.5) * dx[a]);
+        }
+        fprintf(f, "%.6g,", rho);
+        for (int a = 0; a < c.dim; ++a) fprintf(f, "%.6g,", P.vel[a]);
+        fprintf(f, "%.6g,%.6g", P.p, ie);
+        for (int k = 0; k < c.nmat; ++k) fprintf(f, ",%.6g", P.alpha[k]);
+        for (int k = 0; k < c.nmat; ++k) fprintf(f, ",%.6g", P.rho[k]);
+        for (int k = 0; k < c.nmat; ++k) fprintf(f, ",%.6g", U.m[k]);
+        fprintf(f, "\n");
+    }
+    if (fclose(f) != 0) { set_err("dim::write_csv: failed to write file"); return DIMGPU_E_INVALID_ARG; }
+    return 0;
+}

@@ -50,6 +50,10 @@ int oracle_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, const do
 int oracle_solve_line(const dimgpu_desc* d, int n, int dir, double dt, double dx,
                       const double* U_in, double* U_out);
 
+/* dim::write_csv of a SoA field (src/io/dim_write_csv.hpp:15-125). */
+int oracle_write_csv(const dimgpu_desc* d, const double* soa, const double* domain_min,
+                     const double* domain_max, const char* filename);
+
 /* OpenMP threads used by the sweep / CFL loops (<= 0 leaves the default). */
 int oracle_set_threads(int n);
 

@@ -101,6 +101,16 @@ class Checker:
         self._check(self._fn("apply_boundary_conditions")(C.byref(d), dptr(out)), "bc")
         return out
 
+    def write_csv(self, d: Desc, soa, domain_min, domain_max, filename: str) -> None:
+        """dim::write_csv (src/io/dim_write_csv.hpp:15-125) of a SoA field."""
+        soa = np.ascontiguousarray(soa, dtype=np.float64)
+        lo = np.zeros(3)
+        hi = np.zeros(3)
+        lo[:len(domain_min)] = domain_min
+        hi[:len(domain_max)] = domain_max
+        self._check(self._fn("write_csv")(C.byref(d), dptr(soa), dptr(lo), dptr(hi), os.fsencode(filename)),
+                    "write_csv")
+
     def boundary_flux(self, d: Desc, soa) -> np.ndarray:
         """compute_dim_boundary_flux: nmat + dim + 2 values, laid out as totals."""
         soa = np.ascontiguousarray(soa, dtype=np.float64)

@@ -19,6 +19,7 @@
 
 #include "src/app/io/conservation_report.hpp"
 #include "src/dim/solver/advance_step.hpp"
+#include "src/io/dim_write_csv.hpp"
 
 #include "dimgpu.h"
 
@@ -407,6 +408,23 @@ int ref_boundary_flux(const dimgpu_desc* d, const double* soa, double* out)
         out[q++] = t.mass;
         for (int a = 0; a < D; ++a) out[q++] = t.momentum[a];
         out[q++] = t.energy;
+    });)
+    return 0;
+}
+
+// dim::write_csv (src/io/dim_write_csv.hpp:15-125) of a SoA field.
+int ref_write_csv(const dimgpu_desc* d, const double* soa, const double* domain_min, const double* domain_max,
+                  const char* filename)
+{
+    GUARD(DISPATCH_DIM(d, {
+        const auto params = make_params(d);
+        const auto U = load_field<D>(d, soa);
+        std::array<double, D> lo{}, hi{};
+        for (int a = 0; a < D; ++a) {
+            lo[a] = domain_min[a];
+            hi[a] = domain_max[a];
+        }
+        dim::write_csv<D>(filename, U, grid_n<D>(d), lo, hi, params);
     });)
     return 0;
 }

@@ -15,6 +15,17 @@ if ROOT not in sys.path:
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA device and the built libdimgpu.so")
+    config.addinivalue_line("markers", "slow: long CPU stress tests, run only when selected with -m slow")
+
+
+def pytest_collection_modifyitems(config, items):
+    """`slow` tests are opt-in: they run only when the -m expression names them."""
+    if "slow" in (config.getoption("-m") or ""):
+        return
+    skip = pytest.mark.skip(reason="opt-in: select with -m slow")
+    for item in items:
+        if "slow" in item.keywords:
+            item.add_marker(skip)
 
 
 HOST_SO = os.path.join(ROOT, "tests", "_build", "libphyshost.so")

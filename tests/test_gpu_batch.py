@@ -168,3 +168,55 @@ def test_graphs_dropped_when_the_scratch_regrows_in_place(precision):
             out, dts = b.download(iid)
             ref, rdts = _alone(r.desc, r.U, done, 0.6)
             assert ndiff(out, ref) == 0 and bitwise_equal(dts, rdts), r.rid
+
+
+@pytest.mark.parametrize("dim", [1, 2, 3])
+def test_arena_mode_joins_and_leaves_without_allocating(dim):
+    """dimgpu_batch_reserve: after the one reservation, instances join and
+    leave mid-run with no change of the device's free memory, instances that
+    finished early stop being stepped, a full arena refuses with E_OOM, and
+    every result is the instance's own (bit for bit as alone)."""
+    import torch
+
+    if dim == 1:
+        cases = [W.riemann(seed=k, N=(60 + 37 * k,)) for k in range(6)]
+    elif dim == 2:
+        cases = [W.single_bubble_2d((20 + 7 * k, 30 + 5 * k), seed=k) if k % 2 else
+                 W.riemann(seed=k, N=(24 + 9 * k, 18 + 4 * k), axis=k % 2) for k in range(6)]
+    else:
+        cases = [W.bubble_cloud_3d(N=(10 + k, 9 + 2 * k, 8 + k), nbubbles=1 + k % 2, seed=k) for k in range(6)]
+    steps = [7, 19, 3, 26, 11, 16]
+    cfl = 0.5
+    total = sum(d.ncell for d, _ in cases)
+    with Batch(2, dim) as b:
+        b.reserve(max_cells=total // 2 + 64, max_instances=4, max_steps=200)
+        torch.cuda.synchronize()
+        free0, _ = torch.cuda.mem_get_info()
+        ids = {}
+        for k in (0, 1):
+            ids[k] = b.add(cases[k][0], cases[k][1], steps[k], cfl)
+        b.run(5)
+        for k in (2, 3):
+            ids[k] = b.add(cases[k][0], cases[k][1], steps[k], cfl)
+        b.run(9)                                   # instances 0 and 2 finish inside this run
+        outs = {}
+        for k in (0, 2):
+            outs[k] = b.download(ids[k])
+            b.remove(ids.pop(k))
+        for k in (4, 5):
+            try:
+                ids[k] = b.add(cases[k][0], cases[k][1], steps[k], cfl)
+            except DimGpuError as e:
+                assert e.status == abi.E_OOM
+        b.run(40)
+        torch.cuda.synchronize()
+        free1, _ = torch.cuda.mem_get_info()
+        assert free1 == free0
+        for k, iid in ids.items():
+            outs[k] = b.download(iid)
+        used, _ = b.arena_used()
+        assert used == sum(cases[k][0].ncell for k in ids)
+    for k, (out, dts) in outs.items():
+        d, U = cases[k]
+        ref, rdts = _alone(d, U, steps[k], cfl)
+        assert ndiff(out, ref) == 0 and bitwise_equal(dts, rdts), k
