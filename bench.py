@@ -75,6 +75,23 @@ def make_workload(name: str, scale: int = 1):
     raise SystemExit(f"unknown workload {name}")
 
 
+def device_workload(name: str, scale: int = 1):
+    """(desc, init): the workload's descriptor and a function that writes its
+    initial field into a session.  c1 and c2 are generated on the device
+    (dimgpu_init_shock_bubble / dimgpu_init_bubble_cloud, the same bits as
+    the host generators); the others are built on the host and uploaded."""
+    from diffuse_vs_gfm_mms_b200 import workloads as W
+    if name == "c1":
+        d, ic = W.shock_bubble_2d_setup(N=(1024 // scale, 512 // scale))
+        return d, lambda s: s.init_shock_bubble(ic)
+    if name == "c2":
+        n = 512 // scale
+        d, ic, bubbles = W.bubble_cloud_3d_setup(N=(n, n, n), nbubbles=64)
+        return d, lambda s: s.init_bubble_cloud(ic, bubbles)
+    d, U = make_workload(name, scale)
+    return d, lambda s: s.upload(U)
+
+
 def reference_sample(name: str):
     """What the CPU reference runs for a workload: the whole grid wherever
     the reference can hold and step it in seconds (c0, c1, e2); a block of
@@ -349,7 +366,7 @@ def run_ours(args):
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
 
-    d, U = make_workload(args.workload, args.scale)
+    d, init = device_workload(args.workload, args.scale)
     if args.precision == "mixed":
         from diffuse_vs_gfm_mms_b200 import abi as _abi
         d.precision = _abi.PRECISION_MIXED
@@ -361,7 +378,9 @@ def run_ours(args):
     stream = torch.cuda.Stream()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda") if flush_l2 else None
 
-    s = Session(d, U)
+    s = Session(d)
+    init(s)
+    U = s.download() if args.precision == "mixed" else None  # the initial field, for the error analysis
     s.set_stream(stream.cuda_stream)
 
     def barrier():

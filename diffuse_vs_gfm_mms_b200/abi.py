@@ -47,6 +47,7 @@ LAMBDA_MODELS = {"kapila": 0, "": 0, "allaire": 1, "equal_velocity": 2}
 
 PRECISION_FP64 = 0
 PRECISION_MIXED = 1
+PRECISION_MIXED_FP64 = 2   # the mixed algorithm in FP64 throughout (its FP64 twin)
 
 SCHEDULE_FUSED = 0
 SCHEDULE_STAGED = 1

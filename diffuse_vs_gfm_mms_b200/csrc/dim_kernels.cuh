@@ -597,7 +597,7 @@ __global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, __
 // registers allow: the FP64 chains are latency-bound, and the extra warps
 // cut the mixed step's time on a B200 by 2.5 % (2D shock-bubble 1024x512)
 // and 1.2 % (3D bubble cloud 256^3).
-template<int NM, int D, int DIR>
+template<int NM, int D, int DIR, typename R = float>
 __global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
@@ -620,13 +620,13 @@ __global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in,
         Prim<NM, D> lo, hi;
         g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
         g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
-        stage_b_mixed<NM, D>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
+        stage_b_mixed<NM, D, R>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
     }
     g_put<NM, D>(b.Ph, b.cap, t, Ph);
 }
 
 // Face state of cell item t on the given side (end cells: U and P).
-template<int NM, int D, int DIR>
+template<int NM, int D, int DIR, typename R = float>
 __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const Grid& g, const Mats& M,
                                            const StagedBufs<NM, D>& b, const StagedItem<DIR>& it, long long t, int n,
                                            bool right, State<NM, D>& Uf, Prim<NM, D>& Pf)
@@ -641,10 +641,10 @@ __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const 
     g_get<NM, D>(b.Ph, b.cap, t - it.s, lo);
     g_get<NM, D>(b.Ph, b.cap, t, c);
     g_get<NM, D>(b.Ph, b.cap, t + it.s, hi);
-    face_mixed<NM, D>(M, lo, c, hi, right, Uf, Pf);
+    face_mixed<NM, D, R>(M, lo, c, hi, right, Uf, Pf);
 }
 
-template<int NM, int D, int DIR>
+template<int NM, int D, int DIR, typename R = float>
 __global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                    StagedBufs<NM, D> b, int* __restrict__ err)
 {
@@ -655,13 +655,13 @@ __global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in
     if (it.gi >= n - 1) return;  // face i|i+1 exists for i <= n-2
     State<NM, D> UL, UR;
     Prim<NM, D> PL, PR;
-    mixed_face<NM, D, DIR>(in, g, M, b, it, t, n, true, UL, PL);
+    mixed_face<NM, D, DIR, R>(in, g, M, b, it, t, n, true, UL, PL);
     StagedItem<DIR> nx = it;
     nx.gi += 1;
     nx.cell += g.stride[DIR];
-    mixed_face<NM, D, DIR>(in, g, M, b, nx, t + it.s, n, false, UR, PR);
+    mixed_face<NM, D, DIR, R>(in, g, M, b, nx, t + it.s, n, false, UR, PR);
     FaceD<NM, D> f;
-    if (!stage_d_mixed<NM, D>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    if (!stage_d_mixed<NM, D, R>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
     g_put<NM, D>(b.F, b.cap, t, f);
 }
 
@@ -1043,7 +1043,7 @@ cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const dou
 
 template<int NM, int D, int DIR>
 cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, double* out, const double* dt, int* err,
-                             double* scratch, long long cap, const FusedStep& fs, cudaStream_t s)
+                             double* scratch, long long cap, const FusedStep& fs, cudaStream_t s, bool twin)
 {
     const int n = g.N[DIR];
     const long long nlines = g.ncell / n;
@@ -1071,10 +1071,15 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
         mixed_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
         count_launches(1);
         if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
-        mixed_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
-        count_launches(1);
-        mixed_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
-        count_launches(1);
+        if (twin) {
+            mixed_b<NM, D, DIR, double><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+            mixed_cd<NM, D, DIR, double><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+        }
+        else {
+            mixed_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+            mixed_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+        }
+        count_launches(2);
         staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
         count_launches(1);
         const cudaError_t e = cudaGetLastError();
@@ -1086,15 +1091,15 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
 template<int NM, int D>
 cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const double* in, double* out,
                                const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
-                               cudaStream_t s)
+                               cudaStream_t s, bool twin)
 {
     if (fs.on && (long long)g.ncell > cap) return cudaErrorInvalidValue;
-    if (dir == 0) return launch_mixed_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, fs, s);
+    if (dir == 0) return launch_mixed_dir<NM, D, 0>(g, M, in, out, dt, err, scratch, cap, fs, s, twin);
     if constexpr (D >= 2) {
-        if (dir == 1) return launch_mixed_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, fs, s);
+        if (dir == 1) return launch_mixed_dir<NM, D, 1>(g, M, in, out, dt, err, scratch, cap, fs, s, twin);
     }
     if constexpr (D >= 3) {
-        if (dir == 2) return launch_mixed_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, fs, s);
+        if (dir == 2) return launch_mixed_dir<NM, D, 2>(g, M, in, out, dt, err, scratch, cap, fs, s, twin);
     }
     return cudaErrorInvalidValue;
 }
@@ -1276,7 +1281,7 @@ cudaError_t launch_boundary_flux(const Grid& g, const Mats& M, const double* sta
                                                     cudaStream_t);                                           \
     template cudaError_t launch_sweep_mixed<NM, D>(const Grid&, const Mats&, int, const double*, double*,    \
                                                    const double*, int*, double*, long long, const FusedStep&, \
-                                                   cudaStream_t);                                            \
+                                                   cudaStream_t, bool);                                      \
     template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
                                            int, int*, cudaStream_t, bool);                                   \
     template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \

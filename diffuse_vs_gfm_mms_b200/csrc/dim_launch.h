@@ -68,10 +68,12 @@ cudaError_t launch_sweep_staged(const Grid& g, const Mats& M, int dir, const dou
 int staged_scratch_doubles(int nmat, int dim);
 
 // Mixed-precision staged sweep (dim_mixed.h): same scratch as the staged one.
+// twin: the same algorithm with its FP32 quantities in FP64
+// (DIMGPU_PRECISION_MIXED_FP64).
 template<int NM, int D>
 cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const double* in, double* out,
                                const double* dt, int* err, double* scratch, long long cap, const FusedStep& fs,
-                               cudaStream_t s);
+                               cudaStream_t s, bool twin = false);
 
 // Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
 // `mixed`: recover the cells as the mixed-precision step does.

@@ -32,46 +32,61 @@
 namespace dimgpu {
 
 DHD bool finf(float x) { return fabsf(x) <= FLT_MAX; }
-DHD float safe_div_f(float n, float d, float tol = 1e-10f)
+
+// The small-quantity arithmetic is a template over its type R: float is the
+// mixed form; double gives its FP64 twin (DIMGPU_PRECISION_MIXED_FP64), the
+// same algorithm — closed-form recovery, no face round trip, the increment
+// form of HLLC — with every quantity in FP64, so that (mixed - twin) is what
+// FP32 costs and (twin - FP64 step) what the algorithm's shortcuts cost.
+template<typename R>
+DHD bool fin_r(R x)
 {
-    const float nn = finf(n) ? n : 0.0f;
-    float dd = d;
-    if (!finf(d) || fabsf(d) < tol) dd = (d < 0.0f) ? -tol : tol;
+    return fabs((double)x) <= (double)(sizeof(R) == 4 ? FLT_MAX : DBL_MAX);
+}
+template<typename R>
+DHD R safe_div_r(R n, R d)
+{
+    const R tol = (R)1e-10;
+    const R nn = fin_r<R>(n) ? n : (R)0;
+    R dd = d;
+    if (!fin_r<R>(d) || (R)fabs((double)d) < tol) dd = (d < (R)0) ? -tol : tol;
     return nn / dd;
 }
-DHD float minmod_f(float a, float b)
+template<typename R>
+DHD R minmod_r(R a, R b)
 {
-    if (a * b <= 0.0f) return 0.0f;
-    return fabsf(a) < fabsf(b) ? a : b;
+    if (a * b <= (R)0) return (R)0;
+    return fabs((double)a) < fabs((double)b) ? a : b;
 }
 
-// One limited half slope: FP64 differences, FP32 minmod, FP64 half slope.
+// One limited half slope: FP64 differences, minmod in R, FP64 half slope.
+template<typename R = float>
 DHD double half_slope_mixed(double lo, double c, double hi)
 {
-    return 0.5 * (double)minmod_f((float)(c - lo), (float)(hi - c));
+    return 0.5 * (double)minmod_r<R>((R)(c - lo), (R)(hi - c));
 }
 
 // reconstruct_cell_faces with FP32-limited slopes (see the file comment).
-template<int NM, int D>
+template<int NM, int D, typename R = float>
 DHD void reconstruct_mixed(const Prim<NM, D>& PL, const Prim<NM, D>& PC, const Prim<NM, D>& PR, Prim<NM, D>& Lf,
                            Prim<NM, D>& Rf)
 {
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
-        const double h = half_slope_mixed(PL.rho[k], PC.rho[k], PR.rho[k]);
+        const double h = half_slope_mixed<R>(PL.rho[k], PC.rho[k], PR.rho[k]);
         Lf.rho[k] = PC.rho[k] - h;
         Rf.rho[k] = PC.rho[k] + h;
-        const double a = half_slope_mixed(PL.alpha[k], PC.alpha[k], PR.alpha[k]);
+        const double a = half_slope_mixed<R>(PL.alpha[k], PC.alpha[k], PR.alpha[k]);
         Lf.alpha[k] = PC.alpha[k] - a;
         Rf.alpha[k] = PC.alpha[k] + a;
     }
 #pragma unroll
     for (int d = 0; d < D; ++d) {
-        const double h = half_slope_mixed(PL.vel[d], PC.vel[d], PR.vel[d]);
+        const double h = half_slope_mixed<R>(PL.vel[d], PC.vel[d], PR.vel[d]);
         Lf.vel[d] = PC.vel[d] - h;
         Rf.vel[d] = PC.vel[d] + h;
     }
-    const double h = half_slope_mixed(PL.p, PC.p, PR.p);
+    const double h = half_slope_mixed<R>(PL.p, PC.p, PR.p);
     Lf.p = PC.p - h;
     Rf.p = PC.p + h;
     enforce_positive_primitive<NM, D>(Lf);
@@ -164,7 +179,7 @@ DHD void stage_a_mixed(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 // rounding of the increments only.  For mirror states at a wall
 // (p_L = p_R, a_L = -a_R, u_L = -u_R) a_R / (a_L - a_R) is exactly -1/2, s*
 // is exactly 0, and so are the mass and energy fluxes.
-template<int NM, int D>
+template<int NM, int D, typename R = float>
 DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& UR, const Prim<NM, D>& PL,
                     const Prim<NM, D>& PR, int dir, Flux<NM, D>& F, double& s_face)
 {
@@ -181,10 +196,10 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
     const double sL = dmin(unL - cL, unR - cR);
     const double sR = dmax(unL + cL, unR + cR);
 
-    const float aL = (float)(rhoL * (sL - unL)), aR = (float)(rhoR * (sR - unR));
-    const float den = aL - aR;
-    const float w = safe_div_f(aR, den);
-    double s_star = unL + (double)safe_div_f((float)(pR - pL), den) + (double)w * (unL - unR);
+    const R aL = (R)(rhoL * (sL - unL)), aR = (R)(rhoR * (sR - unR));
+    const R den = aL - aR;
+    const R w = safe_div_r<R>(aR, den);
+    double s_star = unL + (double)safe_div_r<R>((R)(pR - pL), den) + (double)w * (unL - unR);
     if (fabs(pL - pR) < 1e-10 && fabs(unL - unR) < 1e-10) s_star = unL;
 
     const bool average = !fin(sL) || !fin(sR) || !fin(s_star);
@@ -196,14 +211,14 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
     const double sK = left ? sL : sR;
     const double unK = left ? unL : unR;
     if (star) {
-        const float ds = (float)(s_star - unK);                   // s* - u_K
-        const float chi_m1 = safe_div_f(ds, (float)(sK - s_star));
+        const R ds = (R)(s_star - unK);                   // s* - u_K
+        const R chi_m1 = safe_div_r<R>(ds, (R)(sK - s_star));
         const double chi = 1.0 + (double)chi_m1;
-        const float sKrK = (float)sK * (float)rhoK;
+        const R sKrK = (R)sK * (R)rhoK;
         const double a = chi * s_star;
         const double E = a * (UK.E + pK + (double)(sKrK * ds));
         s_face = s_star;
-        if (chi > 0.0 && finf(chi_m1) && fin(E)) {
+        if (chi > 0.0 && fin_r<R>(chi_m1) && fin(E)) {
 #pragma unroll
             for (int k = 0; k < NM; ++k) F.m[k] = a * UK.m[k];
 #pragma unroll
@@ -243,7 +258,7 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
 // repair round trip, FP64 Hancock half step (hancock_predict's arithmetic,
 // muscl.hpp:143-191, evaluated face by face as in stage_b) and FP64
 // recovery into Ph.
-template<int NM, int D>
+template<int NM, int D, typename R = float>
 DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
                        const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, Prim<NM, D>& Ph)
 {
@@ -254,7 +269,7 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
     double rhs[NM];
     alpha_rhs_coefficients<NM, D>(M, A.Pe, A.ck, rhs);
     Prim<NM, D> Pl, Pr;
-    reconstruct_mixed<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
+    reconstruct_mixed<NM, D, R>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
     Flux<NM, D> FL, FR;
     {
         State<NM, D> Ul;
@@ -295,29 +310,29 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
 // left) face of a cell from the half-step primitives of the cell and its
 // neighbours (reconstruct_mixed, one side only).  An end cell's face state
 // is its own state U and primitive P instead (as in stage_c).
-template<int NM, int D>
+template<int NM, int D, typename R = float>
 DHD void face_mixed(const Mats& M, const Prim<NM, D>& Ph_lo, const Prim<NM, D>& Ph, const Prim<NM, D>& Ph_hi,
                     bool right, State<NM, D>& Uf, Prim<NM, D>& Pf)
 {
     const double sg = right ? 1.0 : -1.0;
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
-        Pf.rho[k] = Ph.rho[k] + sg * half_slope_mixed(Ph_lo.rho[k], Ph.rho[k], Ph_hi.rho[k]);
-        Pf.alpha[k] = Ph.alpha[k] + sg * half_slope_mixed(Ph_lo.alpha[k], Ph.alpha[k], Ph_hi.alpha[k]);
+        Pf.rho[k] = Ph.rho[k] + sg * half_slope_mixed<R>(Ph_lo.rho[k], Ph.rho[k], Ph_hi.rho[k]);
+        Pf.alpha[k] = Ph.alpha[k] + sg * half_slope_mixed<R>(Ph_lo.alpha[k], Ph.alpha[k], Ph_hi.alpha[k]);
     }
 #pragma unroll
-    for (int d = 0; d < D; ++d) Pf.vel[d] = Ph.vel[d] + sg * half_slope_mixed(Ph_lo.vel[d], Ph.vel[d], Ph_hi.vel[d]);
-    Pf.p = Ph.p + sg * half_slope_mixed(Ph_lo.p, Ph.p, Ph_hi.p);
+    for (int d = 0; d < D; ++d) Pf.vel[d] = Ph.vel[d] + sg * half_slope_mixed<R>(Ph_lo.vel[d], Ph.vel[d], Ph_hi.vel[d]);
+    Pf.p = Ph.p + sg * half_slope_mixed<R>(Ph_lo.p, Ph.p, Ph_hi.p);
     enforce_positive_primitive<NM, D>(Pf);
     prim_to_cons<NM, D>(M, Pf, Uf);
 }
 
 // Stage D of the mixed step: HLLC at face i|i+1 and the upwind alpha flux.
-template<int NM, int D>
+template<int NM, int D, typename R = float>
 DHD bool stage_d_mixed(const Mats& M, const State<NM, D>& UL, const Prim<NM, D>& PL, const State<NM, D>& UR,
                        const Prim<NM, D>& PR, int dir, FaceD<NM, D>& out)
 {
-    const bool ok = hllc_mixed<NM, D>(M, UL, UR, PL, PR, dir, out.F, out.fv);
+    const bool ok = hllc_mixed<NM, D, R>(M, UL, UR, PL, PR, dir, out.F, out.fv);
     const double* up = (out.fv >= 0.0) ? PL.alpha : PR.alpha;
 #pragma unroll
     for (int k = 0; k < NM; ++k) out.af[k] = up[k] * out.fv;

@@ -215,7 +215,7 @@ cudaError_t run_cfl(dimgpu_session* s, double cfl, double dt_max, double* hist)
         else {
             DISPATCH_ND(s->desc.nmat, s->desc.dim,
                         e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks,
-                                              &nb, s->stream, s->desc.precision == DIMGPU_PRECISION_MIXED));
+                                              &nb, s->stream, s->desc.precision != DIMGPU_PRECISION_FP64));
         }
     }
     if (e != cudaSuccess) return e;
@@ -249,13 +249,14 @@ cudaError_t run_sweep(dimgpu_session* s, int dir, const double* in, double* out,
                                                           ends_copy, s->stream));
         return e;
     }
-    if (s->desc.precision == DIMGPU_PRECISION_MIXED) {
+    if (s->desc.precision != DIMGPU_PRECISION_FP64) {
         e = ensure_staged_scratch(s);
         if (e != cudaSuccess) return e;
         ProfScope p(s, kSweep);
+        const bool twin = s->desc.precision == DIMGPU_PRECISION_MIXED_FP64;
         DISPATCH_ND(s->desc.nmat, s->desc.dim,
                     e = launch_sweep_mixed<NM, D>(s->g, s->M, dir, in, out, s->dt, s->err, s->staged,
-                                                  s->staged_cap, fs, s->stream));
+                                                  s->staged_cap, fs, s->stream, twin));
         return e;
     }
     if (s->schedule[dir] == DIMGPU_SCHEDULE_STAGED) {
@@ -338,7 +339,7 @@ cudaError_t run_step(dimgpu_session* s, double cfl, double dt_max, double* hist)
 {
     const bool fusable = !is_euler(s->desc) && s->desc.time_update == DIMGPU_TIME_SPLIT && s->g.N[0] > 1 &&
                          s->cfl_slot &&
-                         (s->desc.precision == DIMGPU_PRECISION_MIXED ||
+                         (s->desc.precision != DIMGPU_PRECISION_FP64 ||
                           s->schedule[0] == DIMGPU_SCHEDULE_STAGED) &&
                          s->ncell <= kStagedChunkCells;
     if (!fusable) {

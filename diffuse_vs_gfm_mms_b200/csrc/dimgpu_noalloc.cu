@@ -139,7 +139,7 @@ extern "C" int dimgpu_compute_dt_cfl_noalloc(const dimgpu_desc* desc, const doub
         switch (desc->nmat * 10 + desc->dim) {
 #define NOALLOC_CASE(NM, D) \
             case NM * 10 + D: e = launch_cfl<NM, D>(g, M, d_state, cfl, unsplit, blockmin, kScratchSlots, &nb, s, \
-                                                    desc->precision == DIMGPU_PRECISION_MIXED); break;
+                                                    desc->precision != DIMGPU_PRECISION_FP64); break;
             NOALLOC_CASE(1, 1) NOALLOC_CASE(1, 2) NOALLOC_CASE(1, 3)
             NOALLOC_CASE(2, 1) NOALLOC_CASE(2, 2) NOALLOC_CASE(2, 3)
             NOALLOC_CASE(3, 1) NOALLOC_CASE(3, 2) NOALLOC_CASE(3, 3)

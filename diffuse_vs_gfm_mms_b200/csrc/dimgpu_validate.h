@@ -38,8 +38,9 @@ inline int check_desc(const dimgpu_desc* d, std::string* msg)
     }
     if (d->lambda_model < 0 || d->lambda_model > 2)
         return bad(DIMGPU_E_INVALID_ARG, "dim::alpha_rhs_coefficients: unknown lambda model");
-    if (d->precision != DIMGPU_PRECISION_FP64 && d->precision != DIMGPU_PRECISION_MIXED)
-        return bad(DIMGPU_E_INVALID_ARG, "precision must be DIMGPU_PRECISION_FP64 or _MIXED");
+    if (d->precision != DIMGPU_PRECISION_FP64 && d->precision != DIMGPU_PRECISION_MIXED &&
+        d->precision != DIMGPU_PRECISION_MIXED_FP64)
+        return bad(DIMGPU_E_INVALID_ARG, "precision must be DIMGPU_PRECISION_FP64, _MIXED or _MIXED_FP64");
     if (d->time_update != DIMGPU_TIME_SPLIT && d->time_update != DIMGPU_TIME_UNSPLIT)
         return bad(DIMGPU_E_INVALID_ARG, "time_update must be split or unsplit");
     if (d->model != DIMGPU_MODEL_DIM && d->model != DIMGPU_MODEL_EULER)

@@ -81,7 +81,10 @@ enum {
 /* Arithmetic of the step. */
 enum {
     DIMGPU_PRECISION_FP64 = 0,  /* bit-faithful to the reference's double run        */
-    DIMGPU_PRECISION_MIXED = 1  /* FP32 reconstruction + HLLC, FP64 state/EoS/dt      */
+    DIMGPU_PRECISION_MIXED = 1, /* FP32 reconstruction + HLLC, FP64 state/EoS/dt      */
+    DIMGPU_PRECISION_MIXED_FP64 = 2  /* the mixed form's algorithm with its FP32 quantities
+                                      * in FP64: (MIXED - this) is the cost of FP32 alone,
+                                      * (this - FP64) the cost of the algorithm's shortcuts */
 };
 
 /* Sweep schedules (results are identical; speed differs by grid shape). */

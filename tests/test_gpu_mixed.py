@@ -136,12 +136,52 @@ def test_mixed_totals_track_fp64():
         assert abs(tmx[q] - t64[q]) <= 1e-9 * abs(t64[q]), (q, t64[q], tmx[q])
 
 
-def test_mixed_changes_nothing_for_the_fp64_path():
+def test_fp64_sessions_unchanged_by_interleaved_mixed_sessions(port):
+    """An FP64 session stepped in between mixed-precision sessions on the
+    same GPU (sharing nothing but the device) stays bit-identical to the
+    oracle: the mixed kernels leave no state behind."""
     d, U = W.shock_bubble_2d(N=(128, 64))
-    with Session(d, U) as s:
-        s.steps(5, 0.8, 1e300)
-        a = s.download()
-    with Session(d, U) as s:
-        s.steps(5, 0.8, 1e300)
-        b = s.download()
-    assert np.array_equal(a, b)
+    dm = d.copy()
+    dm.precision = abi.PRECISION_MIXED
+    with Session(d, U) as s64, Session(dm, U) as smx:
+        for _ in range(3):
+            smx.steps(2, 0.8, 1e300)
+            s64.steps(2, 0.8, 1e300)
+        a = s64.download()
+        m = smx.download()
+    ref, _ = port.advance(d, U, 0.8, 1e300, 6)
+    assert np.array_equal(a, ref)
+    assert not np.array_equal(m, ref)
+
+
+TWIN_CASES = [
+    ("c0 1D riemann 1000, seed 0 (stiffened | ideal)", lambda: W.riemann(seed=0, N=(1000,)), 0.8, 100),
+    ("c0-shaped 1D riemann 1000, seed 2", lambda: W.riemann(seed=2, N=(1000,)), 0.8, 100),
+    ("c0-shaped 1D riemann 1000, seed 3", lambda: W.riemann(seed=3, N=(1000,)), 0.8, 100),
+    ("c1 2D shock-bubble 256x128, 100 steps", lambda: W.shock_bubble_2d(N=(256, 128)), 0.8, 100),
+    ("c1 2D shock-bubble 256x128, 300 steps (after the interaction)",
+     lambda: W.shock_bubble_2d(N=(256, 128)), 0.8, 300),
+    ("c2-shaped 3D cloud 32^3", lambda: W.bubble_cloud_3d(N=(32, 32, 32), nbubbles=6), 0.6, 100),
+]
+
+
+@pytest.mark.parametrize("name,gen,cfl,n", TWIN_CASES)
+def test_fp32_cost_against_the_fp64_twin(port, name, gen, cfl, n):
+    """The mixed form against its FP64 twin (DIMGPU_PRECISION_MIXED_FP64: the
+    same algorithm — closed-form recovery, no face round trip, increment-form
+    HLLC — with its FP32 quantities in FP64).  (mixed - twin) is what FP32
+    costs: it must be within 1e-6 relative L1 on every conserved variable.
+    (twin - oracle) is what the algorithm's shortcuts cost and is printed
+    beside it."""
+    d, U = gen()
+    out, dts = _mixed(d, U, cfl, n)
+    dt_ = d.copy()
+    dt_.precision = abi.PRECISION_MIXED_FP64
+    with Session(dt_, U) as s:
+        tdts = s.steps(n, cfl, 1e300)
+        twin = s.download()
+    ref, rdts = port.advance(d, U, cfl, 1e300, n)
+    fp32 = _report(name + " — mixed vs FP64 twin", out, twin, dts, tdts, d)
+    _report(name + " — FP64 twin vs the FP64 oracle", twin, ref, tdts, rdts, d)
+    assert np.all(np.isfinite(out)) and np.all(np.isfinite(twin))
+    assert np.all(fp32 <= REL_L1_TOL), fp32
