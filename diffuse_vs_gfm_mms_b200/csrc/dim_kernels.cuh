@@ -6,6 +6,8 @@
 // kernel reduces the step; the boundary kernel refills the boundary shell.
 #pragma once
 
+#include <cuda.h>
+#include <cstring>
 #include <cuda_runtime.h>
 
 #include "dim_launch.h"
@@ -130,6 +132,8 @@ __host__ __device__ constexpr int kStateVars(int nm, int d) { return 2 * nm + d;
 // Largest live set between two stages: LS + PLS (stage C -> D).
 __host__ __device__ constexpr int kSweepSmemVars(int nm, int d) { return kStateVars(nm, d) + kPrimVars(nm, d); }
 
+__host__ __device__ constexpr int kStateVarsT(int nm, int d) { return 2 * nm + d; }
+
 // ---- the sweep kernel ------------------------------------------------------------
 //
 // CTA = T*W threads over W lines x T consecutive cells of each line.  For the
@@ -139,12 +143,55 @@ __host__ __device__ constexpr int kSweepSmemVars(int nm, int d) { return kStateV
 // cells tile*(T-6) - 3 + pos; positions 3..T-4 are written, the rest is halo.
 // Stage k+1 of a cell reads stage-k results of its two neighbours from shared
 // memory, so every stage is separated by one __syncthreads.
+//
+// Input staging.  With `tma`, the CTA's whole input tile — its cells plus the
+// 3-cell halo on each side, every component — arrives in shared memory in
+// one TMA copy (cp.async.bulk.tensor, no multicast; the tensor map covers the
+// input buffer of this GPU only), issued by thread 0 and awaited on an
+// mbarrier; each thread then reads its cell from shared memory.  Tensor
+// views (innermost first): x sweep (x, line, component), box (T + 2, W, V),
+// its x start rounded down to an even cell so that it is 16-byte aligned;
+// y sweep (x, y, z, component), box (W, T, 1, V); z sweep box (W, 1, T, V).
+// Cells outside the grid arrive as zeros and are never read.  The wait is
+// bounded: when it runs out, the CTA sets kErrTimeout, waits once more (also
+// bounded) for the copy in flight, and returns without computing.
+struct TileMap {
+    CUtensorMap map;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p)
+{
+    return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// Thread 0 only: bounded wait for phase 0 of the barrier.  True if complete.
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned bar, long long limit)
+{
+    for (long long it = 0; it < limit; ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.test_wait.parity.shared::cta.b64 p, [%1], 0;\n selp.u32 %0, 1, 0, p;\n}"
+            : "=r"(done)
+            : "r"(bar)
+            : "memory");
+        if (done) return true;
+        __nanosleep(64);
+    }
+    return false;
+}
+
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, 2) sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                     __grid_constant__ const Grid g, __grid_constant__ const Mats M, int T, int W, int ntile, int ngx,
-                                                    const double* __restrict__ dtp, int* __restrict__ err)
+                                                    const double* __restrict__ dtp, int* __restrict__ err,
+                                                    const __grid_constant__ TileMap tmap, int tma)
 {
-    extern __shared__ double sm[];
+    extern __shared__ __align__(128) double sm_raw[];
+    constexpr int V = kStateVarsT(NM, D);
+    // TMA tile first (128-byte aligned), stage records after it
+    const int tile_doubles = tma ? ((DIR == 0 ? (T + 2) : T) * W * V + 15) / 16 * 16 : 0;
+    double* tile_sm = sm_raw;
+    double* sm = sm_raw + tile_doubles;
     const int NT = T * W;
     const int t = threadIdx.x;
     const int n = g.N[DIR];
@@ -188,11 +235,83 @@ __global__ void __launch_bounds__(256, 2) sweep_kernel(const double* __restrict_
     const double dt = *dtp;
     const double dx = g.dx[DIR];
 
+    // ---- input tile
+    int xoff = 0;  // x sweep: this tile's first cell minus the aligned box start
+    if (tma) {
+        __shared__ __align__(8) unsigned long long bar;
+        __shared__ int ok;
+        const unsigned bar_a = smem_u32(&bar);
+        if (t == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a) : "memory");
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        }
+        __syncthreads();
+        int c0, c1, c2;  // box start: innermost coordinate first
+        const int x0 = tile * OUT - 3;
+        if (DIR == 0) {
+            const int xa = x0 - (x0 & 1);
+            xoff = x0 - xa;
+            c0 = xa;
+            c1 = (int)((bid / ntile) * W);
+            c2 = 0;
+        }
+        else {
+            const int gx = (int)(bid % ngx);
+            const long long other = (bid / ngx) / ntile;
+            c0 = gx * W;
+            c1 = DIR == 1 ? x0 : (int)other;
+            c2 = DIR == 1 ? (int)other : x0;
+        }
+        if (t == 0) {
+            const unsigned bytes = (unsigned)((DIR == 0 ? (T + 2) : T) * W * V * 8);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar_a), "r"(bytes) : "memory");
+            const unsigned dst = smem_u32(tile_sm);
+            const unsigned long long map = reinterpret_cast<unsigned long long>(&tmap.map);
+            if (DIR == 0)
+                asm volatile(
+                    "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(dst),
+                    "l"(map), "r"(c0), "r"(c1), "r"(0), "r"(bar_a)
+                    : "memory");
+            else
+                asm volatile(
+                    "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                    " [%0], [%1, {%2, %3, %4, %5}], [%6];" ::"r"(dst),
+                    "l"(map), "r"(c0), "r"(c1), "r"(c2), "r"(0), "r"(bar_a)
+                    : "memory");
+            bool done = mbar_wait_bounded(bar_a, 1LL << 22);
+            if (!done) {
+                atomicOr(err, kErrTimeout);
+                mbar_wait_bounded(bar_a, 1LL << 22);
+            }
+            ok = done ? 1 : 0;
+        }
+        __syncthreads();
+        if (!ok) return;
+        mbar_wait_bounded(bar_a, 1);  // complete: this thread's acquire of the tile
+    }
+
     // ---- stage A
     State<NM, D> U;
     CellA<NM, D> A;
     if (valid) {
-        load_cell<NM, D>(in, g.ncell, cell, U);
+        if (tma) {
+            // shared-memory index of component 0 of this thread's cell
+            const int rows = DIR == 0 ? (T + 2) : T;
+            const int i0 = DIR == 0 ? (j * rows + xoff + pos) : (pos * W + j);
+            const int cs = rows * W;  // component stride
+            int q = 0;
+#pragma unroll
+            for (int k = 0; k < NM; ++k) U.m[k] = tile_sm[(q++) * cs + i0];
+#pragma unroll
+            for (int d = 0; d < D; ++d) U.mom[d] = tile_sm[(q++) * cs + i0];
+            U.E = tile_sm[(q++) * cs + i0];
+#pragma unroll
+            for (int k = 0; k < NM - 1; ++k) U.a[k] = tile_sm[(q++) * cs + i0];
+        }
+        else {
+            load_cell<NM, D>(in, g.ncell, cell, U);
+        }
         stage_a<NM, D>(M, U, A);
         sm_put<NM, D>(sm, NT, t, 0, A.Pe);
     }
@@ -935,6 +1054,65 @@ __global__ void __launch_bounds__(256) totals_kernel(const double* __restrict__ 
 }
 
 // ---- launchers ---------------------------------------------------------------------
+// The tensor map of a fused sweep's input tiles (see sweep_kernel), or false
+// where the layout does not allow one: every global stride and the box's
+// innermost extent must be multiples of 16 bytes (even N[0], even cell
+// count, even W for the y / z sweeps) and every box extent at most 256.
+inline bool make_tile_map(const Grid& g, int dir, int V, const double* base, int T, int W, CUtensorMap* out)
+{
+    using EncodeFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static EncodeFn encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<EncodeFn>(fn);
+    }
+    if (!encode) return false;
+    const long long nx = g.N[0], ny = g.N[1], nz = g.N[2];
+    if ((nx & 1) || (g.ncell & 1) || V > 256 || W > 256) return false;
+    if (dir == 0 && T + 2 > 256) return false;
+    if (dir != 0 && ((W & 1) || T > 256)) return false;
+    cuuint64_t dims[4], strides[3];
+    cuuint32_t box[4], estr[4] = {1, 1, 1, 1};
+    cuuint32_t rank;
+    if (dir == 0) {
+        rank = 3;
+        dims[0] = (cuuint64_t)nx;
+        dims[1] = (cuuint64_t)(g.ncell / nx);
+        dims[2] = (cuuint64_t)V;
+        strides[0] = (cuuint64_t)nx * 8;
+        strides[1] = (cuuint64_t)g.ncell * 8;
+        box[0] = (cuuint32_t)(T + 2);
+        box[1] = (cuuint32_t)W;
+        box[2] = (cuuint32_t)V;
+    }
+    else {
+        rank = 4;
+        dims[0] = (cuuint64_t)nx;
+        dims[1] = (cuuint64_t)ny;
+        dims[2] = (cuuint64_t)nz;
+        dims[3] = (cuuint64_t)V;
+        strides[0] = (cuuint64_t)nx * 8;
+        strides[1] = (cuuint64_t)(nx * ny) * 8;
+        strides[2] = (cuuint64_t)g.ncell * 8;
+        box[0] = (cuuint32_t)W;
+        box[1] = (cuuint32_t)(dir == 1 ? T : 1);
+        box[2] = (cuuint32_t)(dir == 2 ? T : 1);
+        box[3] = (cuuint32_t)V;
+    }
+    const CUresult r = encode(out, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, rank, const_cast<double*>(base), dims, strides,
+                              box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 template<int NM, int D, int DIR>
 cudaError_t launch_sweep_dir(const Grid& g, const Mats& M, Tile tile, const double* in, double* out,
                              const double* dt, int* err, cudaStream_t s)
@@ -953,11 +1131,16 @@ cudaError_t launch_sweep_dir(const Grid& g, const Mats& M, Tile tile, const doub
         const long long other = g.ncell / ((long long)g.N[0] * g.N[DIR]);
         nblocks = (long long)ngx * ntile * other;
     }
-    const size_t smem = sizeof(double) * (size_t)kSweepSmemVars(NM, D) * (size_t)(T * W);
+    TileMap tm;
+    std::memset(&tm, 0, sizeof tm);
+    const int V = kStateVarsT(NM, D);
+    const int tma = make_tile_map(g, DIR, V, in, T, W, &tm.map) ? 1 : 0;
+    const size_t tile_doubles = tma ? ((size_t)(DIR == 0 ? (T + 2) : T) * W * V + 15) / 16 * 16 : 0;
+    const size_t smem = sizeof(double) * ((size_t)kSweepSmemVars(NM, D) * (size_t)(T * W) + tile_doubles);
     auto kern = sweep_kernel<NM, D, DIR>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err);
+    kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err, tm, tma);
     count_launches(1);
     return cudaGetLastError();
 }

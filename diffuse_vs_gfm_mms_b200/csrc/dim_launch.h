@@ -15,6 +15,7 @@ namespace dimgpu {
 enum : int {
     kErrNonFinite = 1,  // hllc_flux_normal's require_positive would throw
     kErrDt = 2,         // CFL step is not positive and finite
+    kErrTimeout = 4,    // a bounded wait for a copy into shared memory ran out
 };
 
 // Kernels launched by this library so far, process-wide (read with

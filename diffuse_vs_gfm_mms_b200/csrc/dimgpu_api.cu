@@ -196,6 +196,8 @@ int check_err(dimgpu_session* s)
         if (h & kErrNonFinite)
             return fail(&s->msg, DIMGPU_E_NONFINITE, "dim::hllc_flux_normal: invalid density or pressure (non-finite)");
         if (h & kErrDt) return fail(&s->msg, DIMGPU_E_NONFINITE, "run_dim_case: non-positive timestep");
+        if (h & kErrTimeout)
+            return fail(&s->msg, DIMGPU_E_TIMEOUT, "sweep: the wait for a tile copy into shared memory ran out");
     }
     return DIMGPU_OK;
 }
