@@ -380,6 +380,10 @@ def run_ours(args):
 
     s = Session(d)
     init(s)
+    if args.schedule == "fused":
+        from diffuse_vs_gfm_mms_b200 import abi as _abi
+        for direction in range(d.dim):
+            s.set_schedule(direction, _abi.SCHEDULE_FUSED)
     U = s.download() if args.precision == "mixed" else None  # the initial field, for the error analysis
     s.set_stream(stream.cuda_stream)
 
@@ -500,12 +504,15 @@ def run_ours(args):
     alg_bytes = 2 * V * 8 * ncell  # read + write of the state, per sweep launch
     achieved = alg_bytes / avg_sweep_s / 1e9
     peak, peak_src = measured_peaks()
-    pkey = args.workload + ("-mixed" if args.precision == "mixed" else "")
+    pkey = args.workload + ("-mixed" if args.precision == "mixed" else "") + \
+        ("-fused" if args.schedule == "fused" else "")
     traffic, traffic_src = ncu_traffic(pkey)
     flops_cell, flops_src = ncu_fp64_flops_per_cell(pkey)
     fp64_peak_flops = fp64_peak()
     sched = "mixed staged sweep (mixed_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \
         "staged sweep (staged_a..staged_e)"
+    if args.schedule == "fused" and args.precision != "mixed":
+        sched = "sweep_kernel (fused tile, TMA-staged input)"
     if args.workload in EULER_WORKLOADS:
         sched = "euler_sweep_kernel (fused tile)"
 
@@ -694,6 +701,8 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--scale", type=int, default=1, help="divide the grid sides (profiling runs)")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--schedule", default="staged", choices=["staged", "fused"],
+                    help="sweep schedule of the FP64 step (fused: one tile kernel per sweep)")
     ap.add_argument("--c3-steps", type=int, default=500)
     ap.add_argument("--c3-instances", type=int, default=256)
     ap.add_argument("--c3-sequential", type=int, default=16, help="instances in the sequential sample")

@@ -525,9 +525,13 @@ struct StagedItem {
 };
 
 // Resident blocks of 256 threads per SM that the staged kernels are compiled
-// for (their register budget: 65536 / (256 * blocks)).
+// for (their register budget: 65536 / (256 * blocks), 85 registers at 3).
+// Measured on a B200, 2D shock-bubble 1024x512, FP64: 0.736 ms per step at
+// 2 blocks (112-128 registers), 0.675 at 3, 0.691 at 4 — the stages are
+// latency-bound, and the third block's warps hide more of the dependent
+// FP64 chains than its spills cost.
 #ifndef DIMGPU_STAGED_MINB
-#define DIMGPU_STAGED_MINB 2
+#define DIMGPU_STAGED_MINB 3
 #endif
 
 // Optional CFL reduction fused into stage A of the first sweep of a step:
