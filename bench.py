@@ -645,37 +645,100 @@ def run_batch(args):
         print(json.dumps(line), flush=True)
 
 
+def _fifo_latencies(arrivals, service):
+    """Latencies of a single server that takes requests first come first
+    served: request k starts at max(arrival_k, end of request k-1)."""
+    t, out = 0.0, []
+    for a, w in sorted(zip(arrivals, service)):
+        t = max(t, a) + w
+        out.append(t - a)
+    return np.array(out)
+
+
 def run_serving(args):
-    """Config 4: the continuous-batching server against the sequential plain
-    path on the same request stream, at each arrival rate of --c4-rates."""
+    """Config 4: the continuous-batching server (dimgpu_server_*) against the
+    sequential plain path on the same request stream, at each arrival rate
+    of --c4-rates.
+
+    Served: the whole stream of --c4-requests requests per rate, submitted at
+    their Poisson arrival times, latency from submission to completion.
+    Sequential: each request of a sample (every --c4-seq-every-th) is solved
+    alone through a session and timed with CUDA events; the whole stream's
+    sequential time is estimated from the sample's device time per cell
+    update, per (dimension, precision) class, and its latencies from a
+    first-come-first-served queue of those service times at the same
+    arrivals.  The decomposition says where the sequential time goes: the
+    share of requests that fill the GPU on their own (>= 2^20 cells), whose
+    rate batching cannot raise."""
     import torch
 
     from diffuse_vs_gfm_mms_b200 import serve
+    from diffuse_vs_gfm_mms_b200.dim import Session
 
     world, rank, local = dist_init()
     torch.cuda.set_device(local)
     stream = torch.cuda.Stream()
-    # warm-up: kernels loaded and the batch graphs captured
     warm = serve.make_requests(4, 0.0, seed=1000, steps_range=(16, 16), n1d_range=(256, 256),
                                side2d_range=(128, 128))
     with serve.Server(hbm_budget_bytes=8e9) as srv:
         srv.serve(warm)
     serve.sequential(warm[:1], stream_handle=stream.cuda_stream)
+
+    # sequential sample: device time per cell update by class
+    base = serve.make_requests(args.c4_requests, 1.0, seed=7 + rank)
+    sample = base[::max(1, args.c4_seq_every)]
+    cost = {}
+    for r in sample:
+        with Session(r.desc, r.U) as s:
+            s.set_stream(stream.cuda_stream)
+            a, z = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            s.enqueue_steps(r.steps, r.cfl, r.dt_max)
+            z.record(stream)
+            s.collect()
+            key = (r.desc.dim, r.desc.precision, r.desc.ncell >= (1 << 20))
+            t, cu = cost.get(key, (0.0, 0))
+            cost[key] = (t + a.elapsed_time(z) * 1e-3, cu + r.desc.ncell * r.steps)
+
+    def service(r):
+        key = (r.desc.dim, r.desc.precision, r.desc.ncell >= (1 << 20))
+        if key not in cost:  # class absent from the sample: nearest class of the same dimension
+            key = min(cost, key=lambda k: (k[0] != r.desc.dim, k[1] != r.desc.precision))
+        t, cu = cost[key]
+        return t / cu * r.desc.ncell * r.steps
+
     rows = []
     with ClockSampler(local) as clk:
         for rate in args.c4_rates:
             reqs = serve.make_requests(args.c4_requests, rate, seed=7 + rank)
             with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8) as srv:
                 st = srv.serve(reqs)
-            sq = serve.sequential(reqs, stream_handle=stream.cuda_stream)
             p50, p99 = st.latency_percentiles()
-            q50, q99 = sq.latency_percentiles()
-            rows.append({"rate_per_s": rate, "served": {"solves_per_s": st.solves_per_s, "p50_s": p50, "p99_s": p99,
-                                                        "peak_slots": st.peak_slots,
-                                                        "peak_gb": st.peak_bytes / 1e9},
-                         "sequential_plain": {"solves_per_s": sq.solves_per_s, "p50_s": q50, "p99_s": q99}})
+            svc = [service(r) for r in reqs]
+            arr = [r.arrival for r in reqs]
+            seq_lat = _fifo_latencies(arr, svc)
+            seq_elapsed = float(max(a + lat for a, lat in zip(sorted(arr), seq_lat)))
+            rows.append({"rate_per_s": rate,
+                         "served": {"solves_per_s": st.solves_per_s, "p50_s": p50, "p99_s": p99,
+                                    "elapsed_s": st.elapsed, "peak_slots": st.peak_slots,
+                                    "peak_gb": st.peak_bytes / 1e9, "quanta": st.quanta},
+                         "sequential_plain": {"solves_per_s": len(reqs) / seq_elapsed,
+                                              "p50_s": float(np.percentile(seq_lat, 50)),
+                                              "p99_s": float(np.percentile(seq_lat, 99)),
+                                              "elapsed_s": seq_elapsed}})
     if rank == 0:
         best = max(rows, key=lambda r: r["served"]["solves_per_s"])
+        svc_all = [service(r) for r in base]
+        big = sum(w for r, w in zip(base, svc_all) if r.desc.ncell >= (1 << 20))
+        decomposition = {
+            "sequential_device_s_total": float(sum(svc_all)),
+            "share_in_gpu_filling_requests": float(big / sum(svc_all)),
+            "speedup_ceiling_if_small_requests_were_free": float(sum(svc_all) / big) if big > 0 else None,
+            "sample": f"{len(sample)} of {len(base)} requests run alone (every {max(1, args.c4_seq_every)}th)",
+            "device_s_per_cell_update_by_class": {f"{k[0]}D,{'mixed' if k[1] else 'fp64'},"
+                                                  f"{'>=1M' if k[2] else '<1M'} cells": v[0] / v[1]
+                                                  for k, v in cost.items()},
+        }
         line = {
             "metric": "DIM served solves/s", "value": world * best["served"]["solves_per_s"], "unit": "solves/s",
             "n_gpus": world, "steps": args.c4_requests, "warmup": 1, "ms_per_step": None,
@@ -686,6 +749,7 @@ def run_serving(args):
                        "sample": f"{args.c4_requests} requests per rate of the 10,000-request stream"},
             "rates": rows,
             "speedup_vs_sequential_plain": best["served"]["solves_per_s"] / best["sequential_plain"]["solves_per_s"],
+            "decomposition": decomposition,
             "clocks": clk.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -707,8 +771,9 @@ def main():
     ap.add_argument("--c3-instances", type=int, default=256)
     ap.add_argument("--c3-sequential", type=int, default=16, help="instances in the sequential sample")
     ap.add_argument("--c4-requests", type=int, default=32)
-    ap.add_argument("--c4-rates", type=float, nargs="+", default=[1.0, 4.0])
+    ap.add_argument("--c4-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0])
     ap.add_argument("--c4-slots", type=int, default=128)
+    ap.add_argument("--c4-seq-every", type=int, default=8, help="sequential sample: every k-th request")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
