@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__ tab, c
 #define BATCH_LOOP_END }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) batch_a(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_a(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
@@ -148,7 +148,7 @@ __global__ void __launch_bounds__(256) batch_a(const BInst* __restrict__ tab, co
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) batch_b(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_b(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(256) batch_b(const BInst* __restrict__ tab, co
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) batch_c(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_c(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN
@@ -212,7 +212,7 @@ __global__ void __launch_bounds__(256) batch_c(const BInst* __restrict__ tab, co
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) batch_d(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_d(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b, int* __restrict__ err)
 {
     BATCH_LOOP_BEGIN
@@ -243,7 +243,7 @@ __global__ void __launch_bounds__(256) batch_d(const BInst* __restrict__ tab, co
 // Stage E writes the other buffer; a running instance whose line along DIR
 // is a single cell (no update along that axis) copies its state across.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) batch_e(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_e(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
     BATCH_LOOP_BEGIN

@@ -524,15 +524,6 @@ struct StagedItem {
     }
 };
 
-// Resident blocks of 256 threads per SM that the staged kernels are compiled
-// for (their register budget: 65536 / (256 * blocks), 85 registers at 3).
-// Measured on a B200, 2D shock-bubble 1024x512, FP64: 0.736 ms per step at
-// 2 blocks (112-128 registers), 0.675 at 3, 0.691 at 4 — the stages are
-// latency-bound, and the third block's warps hide more of the dependent
-// FP64 chains than its spills cost.
-#ifndef DIMGPU_STAGED_MINB
-#define DIMGPU_STAGED_MINB 3
-#endif
 
 // Optional CFL reduction fused into stage A of the first sweep of a step:
 // stage A recovers every cell's primitive from the very state the CFL
@@ -811,12 +802,13 @@ __device__ __forceinline__ double warp_min(double v)
 
 template<int NM, int D>
 __global__ void __launch_bounds__(256) cfl_kernel(const double* __restrict__ st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, double cfl,
-                                                  int unsplit, int mixed, double* __restrict__ blockmin)
+                                                  int unsplit, int mixed, double* __restrict__ blockmin,
+                                                  long long begin, long long end)
 {
     __shared__ double red[32];
     double best = HUGE_VAL;
     const long long stride = (long long)gridDim.x * blockDim.x;
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < g.ncell; i += stride) {
+    for (long long i = begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
         State<NM, D> U;
         Prim<NM, D> P;
         load_cell<NM, D>(st, g.ncell, i, U);
@@ -1293,13 +1285,16 @@ cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const doub
 
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
-                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed)
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed, long long begin,
+                       long long end)
 {
-    long long nb = (g.ncell + 255) / 256;
+    if (end < 0) end = g.ncell;
+    long long nb = (end - begin + 255) / 256;
     if (nb > max_blocks) nb = max_blocks;
     if (nb < 1) nb = 1;
     *nblocks = (int)nb;
-    cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, mixed ? 1 : 0, blockmin);
+    cfl_kernel<NM, D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, mixed ? 1 : 0, blockmin,
+                                                   begin, end);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -1470,7 +1465,7 @@ cudaError_t launch_boundary_flux(const Grid& g, const Mats& M, const double* sta
                                                    const double*, int*, double*, long long, const FusedStep&, \
                                                    cudaStream_t, bool);                                      \
     template cudaError_t launch_cfl<NM, D>(const Grid&, const Mats&, const double*, double, bool, double*,   \
-                                           int, int*, cudaStream_t, bool);                                   \
+                                           int, int*, cudaStream_t, bool, long long, long long);             \
     template cudaError_t launch_bc<NM, D>(const Grid&, const Mats&, double*, cudaStream_t);                  \
     template cudaError_t launch_accumulate<NM, D>(const Grid&, const Mats&, double*, const double*,          \
                                                   const double*, cudaStream_t);                              \

@@ -9,6 +9,16 @@
 
 #include "dim_physics.h"
 
+// Resident blocks of 256 threads per SM that the staged kernels are compiled
+// for (their register budget: 65536 / (256 * blocks), 85 registers at 3).
+// Measured on a B200, 2D shock-bubble 1024x512, FP64: 0.736 ms per step at
+// 2 blocks (112-128 registers), 0.675 at 3, 0.691 at 4 — the stages are
+// latency-bound, and the third block's warps hide more of the dependent
+// FP64 chains than its spills cost.
+#ifndef DIMGPU_STAGED_MINB
+#define DIMGPU_STAGED_MINB 3
+#endif
+
 namespace dimgpu {
 
 // Error bits written by the kernels into the session's flag word.
@@ -77,10 +87,12 @@ cudaError_t launch_sweep_mixed(const Grid& g, const Mats& M, int dir, const doub
                                cudaStream_t s, bool twin = false);
 
 // Per-block CFL minima into blockmin[0 .. nblocks-1]; nblocks <= max_blocks.
-// `mixed`: recover the cells as the mixed-precision step does.
+// `mixed`: recover the cells as the mixed-precision step does.  Cells
+// [begin, end) only (end < 0: to the last cell).
 template<int NM, int D>
 cudaError_t launch_cfl(const Grid& g, const Mats& M, const double* state, double cfl, bool unsplit,
-                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed = false);
+                       double* blockmin, int max_blocks, int* nblocks, cudaStream_t s, bool mixed = false,
+                       long long begin = 0, long long end = -1);
 
 // dt = min(dt_max, min(blockmin)), written to dt[0] and hist[0] (hist may be null).
 cudaError_t launch_cfl_finalize(const double* blockmin, int nblocks, double dt_max, double* dt,

@@ -374,6 +374,32 @@ cudaError_t run_step(dimgpu_session* s, double cfl, double dt_max, double* hist)
 
 namespace dimgpu {
 int session_cuda_fail(dimgpu_session* s, cudaError_t e, const char* what) { return cuda_fail(s, e, what); }
+
+cudaError_t session_cfl_range(dimgpu_session* s, double cfl, double dt_max, long long begin, long long end)
+{
+    int nb = 1;
+    cudaError_t e = cudaSuccess;
+    const bool unsplit = s->desc.time_update == DIMGPU_TIME_UNSPLIT;
+    DISPATCH_ND(s->desc.nmat, s->desc.dim,
+                e = launch_cfl<NM, D>(s->g, s->M, s->buf[s->cur], cfl, unsplit, s->blockmin, kMaxCflBlocks, &nb,
+                                      s->stream, s->desc.precision != DIMGPU_PRECISION_FP64, begin, end));
+    if (e != cudaSuccess) return e;
+    return launch_cfl_finalize(s->blockmin, nb, dt_max, s->dt, nullptr, s->err, s->stream);
+}
+
+cudaError_t session_sweep(dimgpu_session* s, int dir)
+{
+    cudaError_t e = cudaSuccess;
+    if (s->g.N[dir] > 1) {
+        e = run_sweep(s, dir, s->buf[s->cur], s->buf[1 - s->cur]);
+        s->cur = 1 - s->cur;
+    }
+    return e;
+}
+
+cudaError_t session_bc(dimgpu_session* s) { return run_bc(s, s->buf[s->cur]); }
+
+int session_check(dimgpu_session* s) { return check_err(s); }
 }  // namespace dimgpu
 
 extern "C" {

@@ -350,7 +350,7 @@ int dimgpu_batch_create(int nmat, int dim, dimgpu_batch** out)
         dimgpu_batch_destroy(b);
         return rc;
     }
-    b->grid = sms * 4;
+    b->grid = sms * DIMGPU_STAGED_MINB;
     b->own_stream = b->stream;
     *out = b;
     return DIMGPU_OK;
@@ -654,7 +654,7 @@ int dimgpu_batch_set_grid(dimgpu_batch* b, int ctas)
     int dev = 0, sms = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    b->grid = ctas ? ctas : sms * 4;
+    b->grid = ctas ? ctas : sms * DIMGPU_STAGED_MINB;
     drop_graphs(b);
     return DIMGPU_OK;
 }

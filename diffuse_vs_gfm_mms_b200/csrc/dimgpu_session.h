@@ -48,4 +48,17 @@ namespace dimgpu {
 int session_fail(dimgpu_session* s, int code, const std::string& msg);
 int session_cuda_fail(dimgpu_session* s, cudaError_t e, const char* what);
 
+// Stream-ordered session operations without a host synchronisation (the
+// slab solver drives several sessions at once with them):
+//  * min(dt_max, CFL minimum over cells [begin, end) of the current state)
+//    into s->dt;
+//  * one sweep along `dir` with the dt held in s->dt on the device (the
+//    current buffer flips);
+//  * the boundary fill of the current state.
+cudaError_t session_cfl_range(dimgpu_session* s, double cfl, double dt_max, long long begin, long long end);
+cudaError_t session_sweep(dimgpu_session* s, int dir);
+cudaError_t session_bc(dimgpu_session* s);
+// Waits for the session's stream and turns its error flag into a status.
+int session_check(dimgpu_session* s);
+
 }  // namespace dimgpu

@@ -236,3 +236,57 @@ def advance_one_step(U: np.ndarray, desc: Desc, cfl: float, dt_max: float,
     check(lib().dimgpu_advance_one_step(C.byref(desc), dptr(U), dptr(out), cfl, dt_max, C.byref(dt),
                                         C.byref(t) if timings else None))
     return StepResult(out, dt.value, _times_dict(t) if timings else {})
+
+
+class Slabs:
+    """One grid decomposed into slabs along its slowest axis, one slab per
+    listed device (dimgpu_slabs_*): bit-identical to a Session on the whole
+    grid.  devices may repeat a device."""
+
+    def __init__(self, desc: Desc, devices, U: np.ndarray | None = None):
+        self.desc = desc.copy()
+        devs = (C.c_int * len(devices))(*devices)
+        h = C.c_void_p()
+        check(lib().dimgpu_slabs_create(C.byref(self.desc), len(devices), devs, C.byref(h)))
+        self._h = h
+        if U is not None:
+            self.upload(U)
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            msg = lib().dimgpu_slabs_last_error(self._h)
+            raise DimGpuError(rc, msg.decode() if msg else "")
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            lib().dimgpu_slabs_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, U: np.ndarray) -> None:
+        U = np.ascontiguousarray(U, dtype=np.float64)
+        self._check(lib().dimgpu_slabs_upload(self._h, dptr(U), U.size))
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.desc.nvar, self.desc.ncell))
+        self._check(lib().dimgpu_slabs_download(self._h, dptr(out), out.size))
+        return out
+
+    def step(self, cfl: float, dt_max: float) -> float:
+        dt = C.c_double()
+        self._check(lib().dimgpu_slabs_step(self._h, cfl, dt_max, C.byref(dt)))
+        return dt.value
+
+    def steps(self, n: int, cfl: float, dt_max: float) -> np.ndarray:
+        return np.array([self.step(cfl, dt_max) for _ in range(n)])

@@ -60,6 +60,12 @@ SIGNATURES = {
     "dimgpu_init_bubble_cloud": ([_S, C.POINTER(abi.BubbleCloudIC), C.POINTER(abi.BubbleIC), C.c_int], C.c_int),
     "dimgpu_csv_write_async": ([_S, C.c_char_p, _DP, _DP, C.c_int, C.POINTER(C.c_void_p)], C.c_int),
     "dimgpu_csv_wait": ([C.c_void_p], C.c_int),
+    "dimgpu_slabs_create": ([_D, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_void_p)], C.c_int),
+    "dimgpu_slabs_destroy": ([C.c_void_p], C.c_int),
+    "dimgpu_slabs_last_error": ([C.c_void_p], C.c_char_p),
+    "dimgpu_slabs_upload": ([C.c_void_p, _DP, C.c_size_t], C.c_int),
+    "dimgpu_slabs_step": ([C.c_void_p, C.c_double, C.c_double, _DP], C.c_int),
+    "dimgpu_slabs_download": ([C.c_void_p, _DP, C.c_size_t], C.c_int),
     "dimgpu_server_create": ([C.POINTER(abi.ServerConfig), C.POINTER(C.c_void_p)], C.c_int),
     "dimgpu_server_destroy": ([C.c_void_p], C.c_int),
     "dimgpu_server_last_error": ([C.c_void_p], C.c_char_p),

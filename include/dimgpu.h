@@ -340,6 +340,29 @@ int dimgpu_batch_arena_used(const dimgpu_batch* b, long long* cells, long long* 
 int dimgpu_batch_enqueue(dimgpu_batch* b, int n);
 int dimgpu_batch_wait(dimgpu_batch* b);
 
+/* ---- one grid over several GPUs --------------------------------------------
+ * Slab decomposition of one DIM grid along its slowest axis (y in 2D, z in
+ * 3D), one slab per listed device, driven from one process; replaces the
+ * reference's MPI slab driver (src/app/dim_mpi_main.cpp:116-124 slabs,
+ * :383-423 halo exchange, :758 MPI_Allreduce of dt).  Each slab holds three
+ * ghost planes per internal cut (the split sweep's reach), refreshed by
+ * device or peer copies before every sweep along the split axis, and dt is
+ * the minimum over the slabs' owned cells: results are bit-identical to one
+ * session on the whole grid.  `devices` may repeat a device (several slabs
+ * on one GPU).  Split steps of the DIM model, 2D and 3D, at least three
+ * planes per slab. */
+typedef struct dimgpu_slabs dimgpu_slabs;
+
+int dimgpu_slabs_create(const dimgpu_desc* desc, int nslabs, const int* devices, dimgpu_slabs** out);
+int dimgpu_slabs_destroy(dimgpu_slabs* L);
+const char* dimgpu_slabs_last_error(const dimgpu_slabs* L);
+/* Whole-grid SoA state in (count = V * ncell of the whole grid). */
+int dimgpu_slabs_upload(dimgpu_slabs* L, const double* soa, size_t count);
+/* One time step of the whole grid (dim::advance_one_step); dt_out may be NULL. */
+int dimgpu_slabs_step(dimgpu_slabs* L, double cfl, double dt_max, double* dt_out);
+/* Whole-grid SoA state out, gathered from the slabs' owned planes. */
+int dimgpu_slabs_download(dimgpu_slabs* L, double* soa, size_t count);
+
 /* ---- the serving loop ----------------------------------------------------
  * Continuous batching of DIM solve requests.  No counterpart in the
  * reference, which runs one case per process (run_dim_case,

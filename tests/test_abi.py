@@ -62,3 +62,28 @@ def test_struct_layout_matches_header(tmp_path):
 def test_components():
     d = abi.make_desc(3, [4, 4, 4], [1, 1, 1], [("ideal_gas", 1.4, 0), ("ideal_gas", 1.6, 0)])
     assert d.nvar == 7 and d.ncell == 64
+
+
+def test_slab_creator_refusals(lib):
+    """dimgpu_slabs_create refuses, before touching a device, what the slab
+    decomposition does not cover: 1D grids, the unsplit update, the Euler
+    model, and slabs thinner than three planes."""
+    import ctypes as C
+
+    def create(d, n):
+        h = C.c_void_p()
+        devs = (C.c_int * n)(*([0] * n))
+        return lib.dimgpu_slabs_create(C.byref(d), n, devs, C.byref(h)), h
+
+    mats = [("ideal_gas", 1.4, 0), ("stiffened_gas", 4.4, 6e8)]
+    rc, h = create(abi.make_desc(1, [64], [1 / 64], mats), 2)
+    assert rc == abi.E_UNSUPPORTED and not h.value
+    d = abi.make_desc(2, [16, 16], [1 / 16, 1 / 16], mats)
+    d.time_update = abi.TIME_UNSPLIT
+    assert create(d, 2)[0] == abi.E_UNSUPPORTED
+    d = abi.make_desc(2, [16, 16], [1 / 16, 1 / 16], mats)
+    d.model = abi.MODEL_EULER
+    assert create(d, 2)[0] == abi.E_UNSUPPORTED
+    d = abi.make_desc(3, [8, 8, 11], [1 / 8] * 3, mats)
+    assert create(d, 4)[0] == abi.E_INVALID_ARG
+    assert create(d, 0)[0] == abi.E_INVALID_ARG
