@@ -137,9 +137,11 @@ def _profile_figure(key: str, workload: str):
     return None, None
 
 
-def ncu_traffic(workload: str):
-    """DRAM bytes (read + write) per sweep (all kernels of one sweep)."""
-    return _profile_figure("traffic_bytes_per_launch", workload)
+def ncu_traffic(workload: str, ncell: int):
+    """DRAM bytes (read + write) per sweep launch (all kernels of one sweep):
+    the committed per-cell figure times the cells of this run."""
+    per_cell, src = _profile_figure("traffic_bytes_per_cell_sweep", workload)
+    return (per_cell * ncell if per_cell else None), src
 
 
 def ncu_fp64_flops_per_cell(workload: str):
@@ -506,7 +508,7 @@ def run_ours(args):
     peak, peak_src = measured_peaks()
     pkey = args.workload + ("-mixed" if args.precision == "mixed" else "") + \
         ("-fused" if args.schedule == "fused" else "")
-    traffic, traffic_src = ncu_traffic(pkey)
+    traffic, traffic_src = ncu_traffic(pkey, ncell)
     flops_cell, flops_src = ncu_fp64_flops_per_cell(pkey)
     fp64_peak_flops = fp64_peak()
     sched = "mixed staged sweep (mixed_a, mixed_b, mixed_cd, staged_e)" if args.precision == "mixed" else \

@@ -43,6 +43,25 @@ namespace dimgpu {
 
 constexpr int kMaxMat = 4;
 
+// Operation counts of a host profiling build: the host harness defines
+// DIMGPU_OPCOUNT(k) to count the events below; every other build compiles
+// the counts away.
+enum OpCount {
+    kOpRecover,       // mixture pressure recoveries
+    kOpDouble,        // doubling steps of the upper bracket
+    kOpCertain,       // bisection steps decided by the certain bracket
+    kOpLiteral,       // literal residual evaluations
+    kOpNotFast,       // recoveries without a certain bracket
+    kOpRepair,        // repair_state calls
+    kOpRepairBisect,  // repair_state "pressure before" recoveries
+    kOpRepairFloor,   // repair_state exact energy floors
+    kOpSound,         // generic mixture sound speeds
+    kOpCountN
+};
+#ifndef DIMGPU_OPCOUNT
+#define DIMGPU_OPCOUNT(k) ((void)0)
+#endif
+
 // ---- constants per material (filled on the host from dimgpu_desc) --------
 struct Mats {
     double gamma[kMaxMat];
@@ -215,6 +234,7 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
+    DIMGPU_OPCOUNT(kOpRecover);
     rho_total = clamp_min(rho_total);
     e = finite_or(e);
     const double target = finite_or(rho_total * e);
@@ -266,6 +286,7 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
         P_fin = 1e290 * rA;
         fast = fin(P_hi) && fin(P_lo);
     }
+    if (!fast) DIMGPU_OPCOUNT(kOpNotFast);
     // status: -1 certainly f < -thresh, +1 certainly f > thresh, 0 unknown
     auto status = [&](double p) -> int {
         if (!fast) return 0;
@@ -285,6 +306,7 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
     if (s < 0) flo_ok = true;
     else if (s > 0) flo_ok = false;
     else {
+        DIMGPU_OPCOUNT(kOpLiteral);
         const double flo = R.literal(M, lo);
         flo_ok = fin(flo) && flo <= 0.0;
     }
@@ -292,12 +314,23 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
     bool fhi_neg, fhi_finite;
     s = status(hi);
     if (s != 0) { fhi_neg = s < 0; fhi_finite = true; }
-    else { const double fhi = R.literal(M, hi); fhi_finite = fin(fhi); fhi_neg = fhi_finite && fhi < 0.0; }
+    else {
+        DIMGPU_OPCOUNT(kOpLiteral);
+        const double fhi = R.literal(M, hi);
+        fhi_finite = fin(fhi);
+        fhi_neg = fhi_finite && fhi < 0.0;
+    }
     for (int n = 0; n < 80 && fhi_finite && fhi_neg; ++n) {
+        DIMGPU_OPCOUNT(kOpDouble);
         hi *= 2.0;
         s = status(hi);
         if (s != 0) { fhi_neg = s < 0; fhi_finite = true; }
-        else { const double fhi = R.literal(M, hi); fhi_finite = fin(fhi); fhi_neg = fhi_finite && fhi < 0.0; }
+        else {
+            DIMGPU_OPCOUNT(kOpLiteral);
+            const double fhi = R.literal(M, hi);
+            fhi_finite = fin(fhi);
+            fhi_neg = fhi_finite && fhi < 0.0;
+        }
     }
     const bool fhi_ok = fhi_finite && !fhi_neg;  // fhi >= 0.0
 
@@ -315,6 +348,7 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
         if (no_clamp) {
             const bool up = mid > P_hi, dn = mid < P_lo;
             if (up || dn) {
+                DIMGPU_OPCOUNT(kOpCertain);
                 hi = up ? mid : hi;
                 lo = dn ? mid : lo;
                 continue;
@@ -324,6 +358,7 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
             const double pc = dmax(mid, 1e-10);
             const bool up = pc > P_hi, dn = pc < P_lo;
             if (up || dn) {
+                DIMGPU_OPCOUNT(kOpCertain);
                 hi = up ? mid : hi;
                 lo = dn ? mid : lo;
                 continue;
@@ -331,9 +366,10 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
         }
         else {
             s = status(mid);
-            if (s > 0) { hi = mid; continue; }
-            if (s < 0) { lo = mid; continue; }
+            if (s > 0) { DIMGPU_OPCOUNT(kOpCertain); hi = mid; continue; }
+            if (s < 0) { DIMGPU_OPCOUNT(kOpCertain); lo = mid; continue; }
         }
+        DIMGPU_OPCOUNT(kOpLiteral);
         const double fmid = R.literal(M, mid);
         if (!fin(fmid)) return clamp_min(fallback_pressure);
         if (fabs(fmid) <= thresh) return clamp_min(mid);
@@ -373,6 +409,7 @@ DNI double generic_mixture_sound_speed_v(const Mats& M, double rho_total, double
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
+    DIMGPU_OPCOUNT(kOpSound);
     if (M.lambda_model == 0) return mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
     double sound_speed[NM], xi[NM];
     double xi_mix = 0.0, inverse_sound_sum = 0.0;
@@ -595,6 +632,7 @@ DHD void alpha_rhs_coefficients(const Mats& M, const Prim<NM, D>& P, const doubl
 template<int NM, int D>
 DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
 {
+    DIMGPU_OPCOUNT(kOpRepair);
     const double mass_floor = 1e-12, p_floor = 1e-12, inactive_alpha_floor = 1e-10;
 #pragma unroll
     for (int k = 0; k < NM; ++k) U.m[k] = dmax(finite_or(U.m[k]), 0.0);
@@ -637,6 +675,7 @@ DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
         }
         const double kinetic_before = 0.5 * rho_before * velocity_squared_before;
         const double internal_before = safe_div(finite_or(U.E, kinetic_before) - kinetic_before, rho_before);
+        DIMGPU_OPCOUNT(kOpRepairBisect);
         pressure_before = dmax(pressure_from_internal_energy<NM>(M, rho_before, internal_before,
                                                                  alpha_full, rho_material_before),
                                p_floor);
@@ -696,6 +735,7 @@ DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
             return U;
         }
     }
+    DIMGPU_OPCOUNT(kOpRepairFloor);
     double velocity_squared = 0.0;
 #pragma unroll
     for (int d = 0; d < D; ++d) {

@@ -7,6 +7,10 @@
 #include <cstring>
 #include <vector>
 
+// Operation counts (dimgpu::OpCount) of everything this harness runs.
+static long long g_opcount[16];
+#define DIMGPU_OPCOUNT(k) (++g_opcount[(k)])
+
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_line.h"
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_mixed.h"
 #include "../../diffuse_vs_gfm_mms_b200/csrc/euler_physics.h"
@@ -454,6 +458,14 @@ int host_euler_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, cons
 int host_sweep_direction(const dimgpu_desc* d, int dir, double dt, const double* in, double* out)
 {
     DISPATCH(d, sweep_impl, d, dir, dt, in, out);
+}
+
+// Copies the operation counts into out[0 .. n) and, if reset, zeroes them.
+int host_opcounts(long long* out, int n, int reset)
+{
+    for (int k = 0; k < n && k < 16; ++k) out[k] = g_opcount[k];
+    if (reset) std::memset(g_opcount, 0, sizeof(g_opcount));
+    return dimgpu::kOpCountN;
 }
 
 }  // extern "C"
