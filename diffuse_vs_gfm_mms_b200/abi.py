@@ -124,7 +124,8 @@ class BubbleCloudIC(C.Structure):
 class ServerConfig(C.Structure):
     """dimgpu_server_config."""
     _fields_ = [("hbm_budget_bytes", C.c_double), ("dim_share", C.c_double * 3), ("max_slots", C.c_int),
-                ("quantum", C.c_int), ("max_steps_per_solve", C.c_int)]
+                ("quantum", C.c_int), ("max_steps_per_solve", C.c_int), ("solo_min_cells", C.c_longlong),
+                ("solo_share", C.c_double), ("solo_slots", C.c_int)]
 
 
 class ServerCounters(C.Structure):

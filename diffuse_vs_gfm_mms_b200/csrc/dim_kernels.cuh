@@ -503,6 +503,30 @@ __device__ __forceinline__ void g_get(const double* b, long long cap, long long 
     for (int k = 0; k < NM; ++k) f.af[k] = b[(v++) * cap + t];
 }
 
+// A face flux record (stage B's face fluxes, kept in the LS / RS slots until
+// stage C writes the face states there).
+template<int NM, int D>
+__device__ __forceinline__ void g_put(double* b, long long cap, long long t, const Flux<NM, D>& F)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) b[(v++) * cap + t] = F.m[k];
+#pragma unroll
+    for (int d = 0; d < D; ++d) b[(v++) * cap + t] = F.mom[d];
+    b[v * cap + t] = F.E;
+}
+
+template<int NM, int D>
+__device__ __forceinline__ void g_get(const double* b, long long cap, long long t, Flux<NM, D>& F)
+{
+    int v = 0;
+#pragma unroll
+    for (int k = 0; k < NM; ++k) F.m[k] = b[(v++) * cap + t];
+#pragma unroll
+    for (int d = 0; d < D; ++d) F.mom[d] = b[(v++) * cap + t];
+    F.E = b[v * cap + t];
+}
+
 // Item t of a chunk: its cell index along the line, its cell in the grid and
 // the scratch stride between neighbours along the line.
 template<int DIR>
@@ -563,19 +587,47 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double
         State<NM, D> U;
         load_cell<NM, D>(in, g.ncell, it.cell, U);
         CellA<NM, D> A;
-        stage_a<NM, D>(M, U, A);
+        stage_a<NM, D, true>(M, U, A);
         g_put<NM, D>(b.P, b.cap, t, A.P);
         g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
-        if (fc.on) best = cfl_candidate<NM, D>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+        if (fc.on) best = cfl_candidate<NM, D, true>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
     }
     if (fc.on) fused_cfl_reduce(best, fc);
 }
 
+// Stage B in two kernels.  staged_bf: one thread per face state (2 per
+// cell; the first half of the items are left faces, the second half right
+// faces): reconstruct, build, repair, flux -> the LS / RS slots.  Each
+// routine has one call site here, so all are inlined.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
-                                                StagedBufs<NM, D> b, const double* __restrict__ dtp)
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bf(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+                                                 StagedBufs<NM, D> b)
+{
+    const long long N = (long long)ls.nl * ls.n;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * N) return;
+    const bool right = t >= N;
+    if (right) t -= N;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    if (it.gi == 0 || it.gi == n - 1 || n < 3) return;  // end cells reconstruct nothing
+    Prim<NM, D> lo, c, hi, Pl, Pr;
+    g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
+    g_get<NM, D>(b.Pe, b.cap, t, c);
+    g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+    reconstruct_cell_faces<NM, D>(lo, c, hi, Pl, Pr);
+    Flux<NM, D> F;
+    face_flux<NM, D, true>(M, right ? Pr : Pl, DIR, F);
+    g_put<NM, D>(right ? b.RS : b.LS, b.cap, t, F);
+}
+
+// staged_bu: one thread per cell, the half-step update from the two face
+// fluxes (the face primitives are reconstructed again: the same values).
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+                                                 StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
@@ -593,45 +645,49 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_b(const double
         load_cell<NM, D>(in, g.ncell, it.cell, U);
 #pragma unroll
         for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
-        Prim<NM, D> lo, hi;
+        Prim<NM, D> lo, hi, Pl, Pr;
         g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
         g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+        reconstruct_cell_faces<NM, D>(lo, A.Pe, hi, Pl, Pr);
+        Flux<NM, D> FL, FR;
+        g_get<NM, D>(b.LS, b.cap, t, FL);
+        g_get<NM, D>(b.RS, b.cap, t, FR);
         State<NM, D> Uh;
-        stage_b<NM, D>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Uh, Ph);
+        stage_b_update<NM, D, true>(M, U, A, Pl, Pr, FL, FR, DIR, *dtp, g.dx[DIR], Uh, Ph);
     }
     g_put<NM, D>(b.Ph, b.cap, t, Ph);
 }
 
+// Stage C: one thread per face state (left faces first, then right faces),
+// all routines inlined.  End cells keep U and its primitive on both sides.
 template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_c(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b)
 {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)ls.nl * ls.n) return;
+    const long long N = (long long)ls.nl * ls.n;
+    long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 2 * N) return;
+    const bool right = t >= N;
+    if (right) t -= N;
     const StagedItem<DIR> it(g, ls, t);
     const int n = ls.n;
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
-    State<NM, D> LS, RS;
-    Prim<NM, D> PLS, PRS;
+    State<NM, D> S;
+    Prim<NM, D> P;
     if (end) {
-        load_cell<NM, D>(in, g.ncell, it.cell, LS);
-        RS = LS;
-        g_get<NM, D>(b.P, b.cap, t, PLS);
-        PRS = PLS;
+        load_cell<NM, D>(in, g.ncell, it.cell, S);
+        g_get<NM, D>(b.P, b.cap, t, P);
     }
     else {
-        CellA<NM, D> A;  // only read for end cells
-        State<NM, D> U;
-        Prim<NM, D> Ph, lo, hi;
+        Prim<NM, D> Ph, lo, hi, Lh, Rh;
         g_get<NM, D>(b.Ph, b.cap, t, Ph);
         g_get<NM, D>(b.Ph, b.cap, t - it.s, lo);
         g_get<NM, D>(b.Ph, b.cap, t + it.s, hi);
-        stage_c<NM, D>(M, U, A, Ph, lo, hi, false, LS, RS, PLS, PRS);
+        reconstruct_cell_faces<NM, D>(lo, Ph, hi, Lh, Rh);
+        face_state<NM, D, true>(M, right ? Rh : Lh, S, P);
     }
-    g_put<NM, D>(b.LS, b.cap, t, LS);
-    g_put<NM, D>(b.RS, b.cap, t, RS);
-    g_put<NM, D>(b.PLS, b.cap, t, PLS);
-    g_put<NM, D>(b.PRS, b.cap, t, PRS);
+    g_put<NM, D>(right ? b.RS : b.LS, b.cap, t, S);
+    g_put<NM, D>(right ? b.PRS : b.PLS, b.cap, t, P);
 }
 
 template<int NM, int D, int DIR>
@@ -649,7 +705,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_d(__grid_const
     g_get<NM, D>(b.LS, b.cap, t + it.s, UR);
     g_get<NM, D>(b.PLS, b.cap, t + it.s, PR);
     FaceD<NM, D> f;
-    if (!stage_d<NM, D>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    if (!stage_d<NM, D, DIMGPU_STAGED_INLINE_DE>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
     g_put<NM, D>(b.F, b.cap, t, f);
 }
 
@@ -673,7 +729,8 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_e(const double
     if (!first) g_get<NM, D>(b.F, b.cap, t - it.s, lo);
     if (!last) g_get<NM, D>(b.F, b.cap, t, hi);
     State<NM, D> Un;
-    stage_e<NM, D>(M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, *dtp, g.dx[DIR], Un);
+    stage_e<NM, D, DIMGPU_STAGED_INLINE_DE>(M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, *dtp,
+                                             g.dx[DIR], Un);
     store_cell<NM, D>(out, g.ncell, it.cell, Un);
 }
 
@@ -1190,9 +1247,12 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
         count_launches(1);
         if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
-        staged_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        const unsigned blocks2 = (unsigned)((2 * items + 255) / 256);
+        staged_bf<NM, D, DIR><<<blocks2, 256, 0, s>>>(g, M, ls, b);
         count_launches(1);
-        staged_c<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b);
+        staged_bu<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        count_launches(1);
+        staged_c<NM, D, DIR><<<blocks2, 256, 0, s>>>(in, g, M, ls, b);
         count_launches(1);
         staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
         count_launches(1);

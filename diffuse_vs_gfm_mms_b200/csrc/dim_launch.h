@@ -9,6 +9,8 @@
 
 #include "dim_physics.h"
 
+struct dimgpu_batch;
+
 // Resident blocks of 256 threads per SM that the staged kernels are compiled
 // for (their register budget: 65536 / (256 * blocks), 85 registers at 3).
 // Measured on a B200, 2D shock-bubble 1024x512, FP64: 0.736 ms per step at
@@ -17,6 +19,12 @@
 // FP64 chains than its spills cost.
 #ifndef DIMGPU_STAGED_MINB
 #define DIMGPU_STAGED_MINB 3
+#endif
+
+// Whether the staged D and E kernels inline their sound speeds and repairs
+// (two call sites each) instead of calling the out-of-line copies.
+#ifndef DIMGPU_STAGED_INLINE_DE
+#define DIMGPU_STAGED_INLINE_DE false
 #endif
 
 namespace dimgpu {
@@ -176,5 +184,9 @@ cudaError_t launch_euler_accumulate(const Grid& g, const Mats& M, double* acc, c
 
 // Message returned by dimgpu_last_error(NULL) on the calling thread.
 void set_sessionless_error(const std::string& msg);
+
+// 1 when every step enqueued on the batch has finished, 0 while steps run
+// (cudaEventQuery; no host synchronisation).
+int batch_ready(::dimgpu_batch* b);
 
 }  // namespace dimgpu

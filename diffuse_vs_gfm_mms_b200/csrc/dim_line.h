@@ -28,6 +28,37 @@
 
 namespace dimgpu {
 
+// Routine selectors: IL = true inlines the routine's body (the staged
+// kernels, which call each routine from one site), false calls its single
+// out-of-line copy (kernels that call it from many sites).
+template<int NM, int D, bool IL>
+DHD Prim<NM, D> c2p(const Mats& M, const State<NM, D>& U)
+{
+    if constexpr (IL) return cons_to_prim_t<NM, D, true>(M, U);
+    else return cons_to_prim_v<NM, D>(M, U);
+}
+
+template<int NM, int D, bool IL>
+DHD State<NM, D> p2c(const Mats& M, const Prim<NM, D>& P)
+{
+    if constexpr (IL) return prim_to_cons_t<NM, D>(M, P);
+    else return prim_to_cons_v<NM, D>(M, P);
+}
+
+template<int NM, int D, bool IL>
+DHD State<NM, D> repair(const Mats& M, const State<NM, D>& U)
+{
+    if constexpr (IL) return repair_state_t<NM, D>(M, U);
+    else return repair_state_v<NM, D>(M, U);
+}
+
+template<int NM, bool IL>
+DHD double sound(const Mats& M, double rho_total, double p, const double* alpha, const double* rho)
+{
+    if constexpr (IL) return sound_speed_generic<NM>(M, rho_total, p, mix_of<NM>(alpha, rho));
+    else return generic_mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
+}
+
 template<int NM, int D>
 struct CellA {
     Prim<NM, D> P;   // cons_to_prim(U): un-enforced (primitive[i] in solve_line)
@@ -36,10 +67,10 @@ struct CellA {
 };
 
 // Stage A.
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD void stage_a(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 {
-    cons_to_prim<NM, D>(M, U, A.P);
+    A.P = c2p<NM, D, IL>(M, U);
     A.Pe = A.P;
     enforce_positive_primitive<NM, D>(A.Pe);
     rhs_sound_speeds<NM, D>(M, A.P, A.ck);
@@ -49,36 +80,27 @@ DHD void stage_a(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 // every cell of a line shorter than 3 (no reconstruction there,
 // muscl.hpp:213-226, 244-252, 271-272).  hancock_predict's arithmetic
 // (muscl.hpp:143-191) is evaluated face by face: each face state is built,
-// repaired and turned into its flux before the other one, so a face state
-// is dead before the next out-of-line call (the same operations on the same
-// values; only independent work is reordered).
-template<int NM, int D>
-DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
-                 const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, State<NM, D>& Uh,
-                 Prim<NM, D>& Ph)
+// repaired and turned into its flux (face_flux), then the cell's half-step
+// update combines the two fluxes (stage_b_update) — the same operations on
+// the same values; only independent work is reordered.  The staged kernels
+// run face_flux as one thread per face state and stage_b_update as one
+// thread per cell.
+template<int NM, int D, bool IL = false>
+DHD void face_flux(const Mats& M, const Prim<NM, D>& Pf, int dir, Flux<NM, D>& F)
 {
-    if (end) {
-        Uh = U;
-        Ph = A.Pe;
-        return;
-    }
+    const State<NM, D> Uf = repair<NM, D, IL>(M, p2c<NM, D, IL>(M, Pf));
+    flux_normal<NM, D>(Uf, Pf, dir, F);
+}
+
+// The half-step update of stage B from the cell's face primitives Pl, Pr
+// and their fluxes FL, FR.
+template<int NM, int D, bool IL = false>
+DHD void stage_b_update(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pl,
+                        const Prim<NM, D>& Pr, const Flux<NM, D>& FL, const Flux<NM, D>& FR, int dir, double dt,
+                        double dx, State<NM, D>& Uh, Prim<NM, D>& Ph)
+{
     double rhs[NM];
     alpha_rhs_coefficients<NM, D>(M, A.Pe, A.ck, rhs);
-    Prim<NM, D> Pl, Pr;
-    reconstruct_cell_faces<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
-    Flux<NM, D> FL, FR;
-    {
-        State<NM, D> Ul;
-        prim_to_cons<NM, D>(M, Pl, Ul);
-        repair_state<NM, D>(M, Ul);
-        flux_normal<NM, D>(Ul, Pl, dir, FL);
-    }
-    {
-        State<NM, D> Ur;
-        prim_to_cons<NM, D>(M, Pr, Ur);
-        repair_state<NM, D>(M, Ur);
-        flux_normal<NM, D>(Ur, Pr, dir, FR);
-    }
     const double factor = 0.5 * dt / dx;
     Uh = U;
 #pragma unroll
@@ -99,9 +121,37 @@ DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
     sanitise_alpha<NM>(alpha_new, 0.0);
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) Uh.a[k] = alpha_new[k];
-    repair_state<NM, D>(M, Uh);
-    cons_to_prim<NM, D>(M, Uh, Ph);
+    Uh = repair<NM, D, IL>(M, Uh);
+    Ph = c2p<NM, D, IL>(M, Uh);
     enforce_positive_primitive<NM, D>(Ph);
+}
+
+template<int NM, int D>
+DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
+                 const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, State<NM, D>& Uh,
+                 Prim<NM, D>& Ph)
+{
+    if (end) {
+        Uh = U;
+        Ph = A.Pe;
+        return;
+    }
+    Prim<NM, D> Pl, Pr;
+    reconstruct_cell_faces<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
+    Flux<NM, D> FL, FR;
+    face_flux<NM, D>(M, Pl, dir, FL);
+    face_flux<NM, D>(M, Pr, dir, FR);
+    stage_b_update<NM, D>(M, U, A, Pl, Pr, FL, FR, dir, dt, dx, Uh, Ph);
+}
+
+// One face state of stage C: the conservative state of the reconstructed
+// half-step primitive Pf, repaired, and its primitive.  The staged kernel
+// runs it as one thread per face state.
+template<int NM, int D, bool IL = false>
+DHD void face_state(const Mats& M, const Prim<NM, D>& Pf, State<NM, D>& S, Prim<NM, D>& P)
+{
+    S = repair<NM, D, IL>(M, p2c<NM, D, IL>(M, Pf));
+    P = c2p<NM, D, IL>(M, S);
 }
 
 // Stage C: the half-step face states of cell i (U_left_half[i],
@@ -121,12 +171,8 @@ DHD void stage_c(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
     }
     Prim<NM, D> Lh, Rh;
     reconstruct_cell_faces<NM, D>(Ph_lo, Ph, Ph_hi, Lh, Rh);
-    prim_to_cons<NM, D>(M, Lh, LS);
-    prim_to_cons<NM, D>(M, Rh, RS);
-    repair_state<NM, D>(M, LS);
-    repair_state<NM, D>(M, RS);
-    cons_to_prim<NM, D>(M, LS, PLS);
-    cons_to_prim<NM, D>(M, RS, PRS);
+    face_state<NM, D>(M, Lh, LS, PLS);
+    face_state<NM, D>(M, Rh, RS, PRS);
 }
 
 // Stage D output per face.
@@ -138,11 +184,11 @@ struct FaceD {
 };
 
 // Stage D: face between cell i (UL = RS_i) and cell i+1 (UR = LS_{i+1}).
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD bool stage_d(const Mats& M, const State<NM, D>& UL, const Prim<NM, D>& PL, const State<NM, D>& UR,
                  const Prim<NM, D>& PR, int dir, FaceD<NM, D>& out)
 {
-    const bool ok = hllc_flux<NM, D>(M, UL, UR, PL, PR, dir, out.F, out.fv);
+    const bool ok = hllc_flux<NM, D, IL>(M, UL, UR, PL, PR, dir, out.F, out.fv);
     const double* up = (out.fv >= 0.0) ? PL.alpha : PR.alpha;
 #pragma unroll
     for (int k = 0; k < NM; ++k) out.af[k] = up[k] * out.fv;
@@ -154,7 +200,7 @@ DHD bool stage_d(const Mats& M, const State<NM, D>& UL, const Prim<NM, D>& PL, c
 // i|i+1; first / last mark the line's end cells, whose outer face copies the
 // inner one (F[0] = F[1], F[n] = F[n-1]) and whose outer alpha flux is the
 // cell-centred fraction times that face velocity.
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const FaceD<NM, D>* lo,
                  const FaceD<NM, D>* hi, bool first, bool last, double dt, double dx, State<NM, D>& out)
 {
@@ -189,21 +235,21 @@ DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
     }
     sanitise_alpha<NM>(alpha_new, 0.0);
 
-    repair_state<NM, D>(M, out);
+    out = repair<NM, D, IL>(M, out);
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) out.a[k] = alpha_new[k];
-    repair_state<NM, D>(M, out);
+    out = repair<NM, D, IL>(M, out);
 }
 
 // CFL candidate of one cell (dim::compute_dt_cfl body, src/dim/solver/cfl.hpp:
 // 46-62, and the unsplit variant :94-115): the smallest cfl*dx_d/wave_speed
 // over the axes (or cfl/spectral_sum); +inf when no axis contributes.
 // P = cons_to_prim(U).
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD double cfl_candidate(const Mats& M, const State<NM, D>& U, const Prim<NM, D>& P, const double* dx,
                          double cfl, bool unsplit)
 {
-    const double c = generic_mixture_sound_speed<NM>(M, total_density<NM, D>(U), P.p, P.alpha, P.rho);
+    const double c = sound<NM, IL>(M, total_density<NM, D>(U), P.p, P.alpha, P.rho);
     double best = HUGE_VAL;
     if (unsplit) {
         double spectral_sum = 0.0;

@@ -30,7 +30,11 @@
 // record passed by reference or pointer must live in addressable (local)
 // memory, which turns every call into local stores and loads; by value it
 // stays in registers.  Inline wrappers with the by-reference signatures sit
-// in front of them.
+// in front of them.  Each out-of-line copy wraps an always-inlined body
+// (pressure_recover, sound_speed_generic, cons_to_prim_t, prim_to_cons_t,
+// repair_state_t): a kernel that calls a routine from one site only (the
+// staged sweep's per-face-state kernels) inlines the body and pays no call
+// (no argument moves, no callee-saved registers spilled to local memory).
 #ifdef __CUDACC__
 #define DHD __host__ __device__ __forceinline__
 #define DNI __host__ __device__ __noinline__
@@ -56,10 +60,12 @@ enum OpCount {
     kOpRepairBisect,  // repair_state "pressure before" recoveries
     kOpRepairFloor,   // repair_state exact energy floors
     kOpSound,         // generic mixture sound speeds
+    kOpDoubleSkipped, // doubling steps skipped in one step (bracket-decided)
     kOpCountN
 };
 #ifndef DIMGPU_OPCOUNT
 #define DIMGPU_OPCOUNT(k) ((void)0)
+#define DIMGPU_OPCOUNT_ADD(k, n) ((void)0)
 #endif
 
 // ---- constants per material (filled on the host from dimgpu_desc) --------
@@ -230,7 +236,7 @@ DHD MixVec<NM> mix_of(const double* alpha, const double* rho)
 }
 
 template<int NM>
-DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, double e, MixVec<NM> x)
+DHD double pressure_recover(const Mats& M, double rho_total, double e, MixVec<NM> x)
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
@@ -320,7 +326,21 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
         fhi_finite = fin(fhi);
         fhi_neg = fhi_finite && fhi < 0.0;
     }
-    for (int n = 0; n < 80 && fhi_finite && fhi_neg; ++n) {
+    // Doublings the bracket decides (hi * 2^n < min(P_lo, P_fin): status -1)
+    // are skipped in one step: hi * 2^n is exact, and the first n with
+    // hi * 2^n >= Q is ilogb(Q) - ilogb(hi) or one more (hi >= 1 and Q > hi
+    // are normal numbers here).  The loop resumes at that doubling, with the
+    // same 80-doubling cap.
+    int n0 = 0;
+    if (s < 0) {
+        const double Q = dmin(P_lo, P_fin);
+        int m = ilogb(Q) - ilogb(hi);
+        if (ldexp(hi, m) < Q) ++m;
+        n0 = m - 1 < 80 ? m - 1 : 80;
+        hi = ldexp(hi, n0);
+        DIMGPU_OPCOUNT_ADD(kOpDoubleSkipped, n0);
+    }
+    for (int n = n0; n < 80 && fhi_finite && fhi_neg; ++n) {
         DIMGPU_OPCOUNT(kOpDouble);
         hi *= 2.0;
         s = status(hi);
@@ -380,6 +400,12 @@ DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, doub
 }
 
 template<int NM>
+DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, double e, MixVec<NM> x)
+{
+    return pressure_recover<NM>(M, rho_total, e, x);
+}
+
+template<int NM>
 DHD double pressure_from_internal_energy(const Mats& M, double rho_total, double e, const double* alpha,
                                          const double* rho)
 {
@@ -405,7 +431,7 @@ DHD double mixture_sound_speed(const Mats& M, double rho_total, double p, const 
 
 // MixtureEOS::generic_mixture_sound_speed, src/dim/eos.hpp:223-275
 template<int NM>
-DNI double generic_mixture_sound_speed_v(const Mats& M, double rho_total, double p, MixVec<NM> x)
+DHD double sound_speed_generic(const Mats& M, double rho_total, double p, MixVec<NM> x)
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
@@ -434,6 +460,12 @@ DNI double generic_mixture_sound_speed_v(const Mats& M, double rho_total, double
         rho_c_squared += lambda_k * alpha_k * xi[k] * sound_speed[k] * sound_speed[k] / xi_mix;
     }
     return sqrt(dmax(rho_c_squared / clamp_min(rho_total), 1e-14));
+}
+
+template<int NM>
+DNI double generic_mixture_sound_speed_v(const Mats& M, double rho_total, double p, MixVec<NM> x)
+{
+    return sound_speed_generic<NM>(M, rho_total, p, x);
 }
 
 template<int NM>
@@ -491,8 +523,8 @@ DHD double total_density(const State<NM, D>& U)
 }
 
 // cons_to_prim, primitives.hpp:111-162
-template<int NM, int D>
-DNI Prim<NM, D> cons_to_prim_v(const Mats& M, State<NM, D> U)
+template<int NM, int D, bool IL>
+DHD Prim<NM, D> cons_to_prim_t(const Mats& M, State<NM, D> U)
 {
     Prim<NM, D> P;
     full_alpha<NM, D>(U, P.alpha);
@@ -514,8 +546,17 @@ DNI Prim<NM, D> cons_to_prim_v(const Mats& M, State<NM, D> U)
     }
     const double kinetic = 0.5 * rho_total * velocity_squared;
     const double internal_energy = safe_div(finite_or(U.E, kinetic) - kinetic, rho_total);
-    P.p = dmax(pressure_from_internal_energy<NM>(M, rho_total, internal_energy, P.alpha, P.rho), 1e-12);
+    double p;
+    if constexpr (IL) p = pressure_recover<NM>(M, rho_total, internal_energy, mix_of<NM>(P.alpha, P.rho));
+    else p = pressure_from_internal_energy<NM>(M, rho_total, internal_energy, P.alpha, P.rho);
+    P.p = dmax(p, 1e-12);
     return P;
+}
+
+template<int NM, int D>
+DNI Prim<NM, D> cons_to_prim_v(const Mats& M, State<NM, D> U)
+{
+    return cons_to_prim_t<NM, D, false>(M, U);
 }
 
 template<int NM, int D>
@@ -527,7 +568,7 @@ DHD void cons_to_prim(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
 // prim_to_cons, primitives.hpp:165-212 (internal_energy_from_pressure,
 // src/dim/eos.hpp:146-166, inlined)
 template<int NM, int D>
-DNI State<NM, D> prim_to_cons_v(const Mats& M, Prim<NM, D> P)
+DHD State<NM, D> prim_to_cons_t(const Mats& M, Prim<NM, D> P)
 {
     State<NM, D> U;
     sanitise_alpha<NM>(P.alpha, 1e-12);
@@ -551,6 +592,12 @@ DNI State<NM, D> prim_to_cons_v(const Mats& M, Prim<NM, D> P)
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) U.a[k] = P.alpha[k];
     return U;
+}
+
+template<int NM, int D>
+DNI State<NM, D> prim_to_cons_v(const Mats& M, Prim<NM, D> P)
+{
+    return prim_to_cons_t<NM, D>(M, P);
 }
 
 template<int NM, int D>
@@ -630,7 +677,7 @@ DHD void alpha_rhs_coefficients(const Mats& M, const Prim<NM, D>& P, const doubl
 
 // repair_state, primitives.hpp:325-457.
 template<int NM, int D>
-DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
+DHD State<NM, D> repair_state_t(const Mats& M, State<NM, D> U)
 {
     DIMGPU_OPCOUNT(kOpRepair);
     const double mass_floor = 1e-12, p_floor = 1e-12, inactive_alpha_floor = 1e-10;
@@ -755,6 +802,12 @@ DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
 }
 
 template<int NM, int D>
+DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U)
+{
+    return repair_state_t<NM, D>(M, U);
+}
+
+template<int NM, int D>
 DHD void repair_state(const Mats& M, State<NM, D>& U)
 {
     U = repair_state_v<NM, D>(M, U);
@@ -865,7 +918,7 @@ DHD void hancock_predict(const Mats& M, const State<NM, D>& Uc, const Prim<NM, D
 // PL / PR are cons_to_prim(UL) / cons_to_prim(UR), computed by the caller
 // once per face state.  Returns false where the reference's require_positive
 // throws (non-finite density or pressure, hllc.hpp:88-91).
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD bool hllc_flux(const Mats& M, const State<NM, D>& UL, const State<NM, D>& UR, const Prim<NM, D>& PL,
                    const Prim<NM, D>& PR, int dir, Flux<NM, D>& F, double& s_face)
 {
@@ -882,8 +935,15 @@ DHD bool hllc_flux(const Mats& M, const State<NM, D>& UL, const State<NM, D>& UR
 #pragma unroll
     for (int d = 0; d < D; ++d) unR += PR.vel[d] * (d == dir ? 1.0 : 0.0);
 
-    const double cL = generic_mixture_sound_speed<NM>(M, rhoL, pL, PL.alpha, PL.rho);
-    const double cR = generic_mixture_sound_speed<NM>(M, rhoR, pR, PR.alpha, PR.rho);
+    double cL, cR;
+    if constexpr (IL) {
+        cL = sound_speed_generic<NM>(M, rhoL, pL, mix_of<NM>(PL.alpha, PL.rho));
+        cR = sound_speed_generic<NM>(M, rhoR, pR, mix_of<NM>(PR.alpha, PR.rho));
+    }
+    else {
+        cL = generic_mixture_sound_speed<NM>(M, rhoL, pL, PL.alpha, PL.rho);
+        cR = generic_mixture_sound_speed<NM>(M, rhoR, pR, PR.alpha, PR.rho);
+    }
     const double sL = dmin(unL - cL, unR - cR);
     const double sR = dmax(unL + cL, unR + cR);
     const double numerator = (pR - pL) + rhoL * unL * (sL - unL) - rhoR * unR * (sR - unR);

@@ -402,23 +402,11 @@ cudaError_t session_bc(dimgpu_session* s) { return run_bc(s, s->buf[s->cur]); }
 int session_check(dimgpu_session* s) { return check_err(s); }
 }  // namespace dimgpu
 
-extern "C" {
+namespace {
 
-int dimgpu_components(const dimgpu_desc* desc) { return desc ? 2 * desc->nmat + desc->dim : 0; }
-
-const char* dimgpu_last_error(const dimgpu_session* s)
+// Grid, materials and tile defaults of a session from its descriptor.
+void init_geometry(dimgpu_session* s, const dimgpu_desc* desc)
 {
-    if (s) return s->msg.c_str();
-    return g_err.c_str();
-}
-
-int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
-{
-    if (!out) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null output pointer");
-    *out = nullptr;
-    int rc = validate_desc(desc, nullptr);
-    if (rc) return rc;
-    auto* s = new dimgpu_session();
     s->desc = *desc;
     int kind[kMaxMat];
     double gam[kMaxMat], pinf[kMaxMat];
@@ -452,12 +440,13 @@ int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
         if (desc->dim == 2 && desc->N[0] >= 4) s->tile[1] = {128, 2};
         if (desc->dim == 3) s->tile[0] = {64, 2};
     }
+}
 
-    const size_t bytes = sizeof(double) * (size_t)s->V * (size_t)s->ncell;
+// The session's stream and small device buffers (everything but the grid).
+cudaError_t alloc_small(dimgpu_session* s)
+{
     cudaError_t e = cudaStreamCreateWithFlags(&s->own_stream, cudaStreamNonBlocking);
     s->stream = s->own_stream;
-    const int nbuf = desc->time_update == DIMGPU_TIME_UNSPLIT ? 3 : 2;
-    for (int b = 0; b < nbuf && e == cudaSuccess; ++b) e = cudaMalloc(&s->buf[b], bytes);
     if (e == cudaSuccess) e = cudaMalloc(&s->blockmin, sizeof(double) * kMaxCflBlocks);
     if (e == cudaSuccess) e = cudaMalloc(&s->dt, sizeof(double) * 2);
     if (e == cudaSuccess) e = cudaMalloc(&s->hist, sizeof(double) * kHistCap);
@@ -465,10 +454,95 @@ int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
     if (e == cudaSuccess) e = cudaMalloc(&s->err, sizeof(int));
     if (e == cudaSuccess) e = cudaMalloc(&s->cfl_slot, sizeof(unsigned long long));
     if (e == cudaSuccess) {
-        const double inf = HUGE_VAL;
+        static const double inf = HUGE_VAL;
         e = cudaMemcpyAsync(s->cfl_slot, &inf, sizeof inf, cudaMemcpyHostToDevice, s->stream);
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+    return e;
+}
+
+}  // namespace
+
+namespace dimgpu {
+
+long long session_grid_doubles(const dimgpu_desc* d)
+{
+    long long ncell = 1;
+    for (int a = 0; a < 3; ++a) ncell *= d->N[a];
+    const long long V = 2 * d->nmat + d->dim;
+    const long long nbuf = d->time_update == DIMGPU_TIME_UNSPLIT ? 3 : 2;
+    long long cap = ncell < kStagedChunkCells ? ncell : kStagedChunkCells;
+    for (int a = 0; a < 3; ++a)
+        if (d->N[a] > cap) cap = d->N[a];
+    return nbuf * V * ncell + (long long)staged_scratch_doubles(d->nmat, d->dim) * cap;
+}
+
+int session_shell_create(dimgpu_session** out)
+{
+    if (!out) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null output pointer");
+    auto* s = new dimgpu_session();
+    s->borrowed = true;
+    cudaError_t e = alloc_small(s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    if (e != cudaSuccess) {
+        const int rc = cuda_fail(nullptr, e, "session_shell_create");
+        dimgpu_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return DIMGPU_OK;
+}
+
+int session_shell_bind(dimgpu_session* s, const dimgpu_desc* desc, double* mem)
+{
+    int rc = validate_desc(desc, nullptr);
+    if (rc) return rc;
+    if (!s || !s->borrowed || !mem) return fail(nullptr, DIMGPU_E_INVALID_ARG, "session_shell_bind: bad argument");
+    s->tile[0] = {128, 1};
+    s->tile[1] = {64, 4};
+    s->tile[2] = {64, 4};
+    for (int a = 0; a < 3; ++a) s->schedule[a] = DIMGPU_SCHEDULE_STAGED;
+    init_geometry(s, desc);
+    const int nbuf = desc->time_update == DIMGPU_TIME_UNSPLIT ? 3 : 2;
+    const size_t n = (size_t)s->V * (size_t)s->ncell;
+    for (int b = 0; b < 3; ++b) s->buf[b] = b < nbuf ? mem + (size_t)b * n : nullptr;
+    long long cap = s->ncell < kStagedChunkCells ? s->ncell : kStagedChunkCells;
+    for (int a = 0; a < 3; ++a)
+        if (s->g.N[a] > cap) cap = s->g.N[a];
+    s->staged = mem + (size_t)nbuf * n;
+    s->staged_cap = cap;
+    s->cur = 0;
+    s->pending = 0;
+    s->msg.clear();
+    cudaError_t e = cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return cuda_fail(s, e, "session_shell_bind");
+    return DIMGPU_OK;
+}
+
+}  // namespace dimgpu
+
+extern "C" {
+
+int dimgpu_components(const dimgpu_desc* desc) { return desc ? 2 * desc->nmat + desc->dim : 0; }
+
+const char* dimgpu_last_error(const dimgpu_session* s)
+{
+    if (s) return s->msg.c_str();
+    return g_err.c_str();
+}
+
+int dimgpu_create(const dimgpu_desc* desc, dimgpu_session** out)
+{
+    if (!out) return fail(nullptr, DIMGPU_E_INVALID_ARG, "null output pointer");
+    *out = nullptr;
+    int rc = validate_desc(desc, nullptr);
+    if (rc) return rc;
+    auto* s = new dimgpu_session();
+    init_geometry(s, desc);
+    const size_t bytes = sizeof(double) * (size_t)s->V * (size_t)s->ncell;
+    cudaError_t e = alloc_small(s);
+    const int nbuf = desc->time_update == DIMGPU_TIME_UNSPLIT ? 3 : 2;
+    for (int b = 0; b < nbuf && e == cudaSuccess; ++b) e = cudaMalloc(&s->buf[b], bytes);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
     if (e != cudaSuccess) {
         rc = cuda_fail(nullptr, e, "dimgpu_create");
@@ -488,13 +562,15 @@ int dimgpu_destroy(dimgpu_session* s)
         cudaEventDestroy(r.b);
     }
     for (auto ev : s->pool) cudaEventDestroy(ev);
-    for (int b = 0; b < 3; ++b) cudaFree(s->buf[b]);
+    if (!s->borrowed) {
+        for (int b = 0; b < 3; ++b) cudaFree(s->buf[b]);
+        cudaFree(s->staged);
+    }
     cudaFree(s->blockmin);
     cudaFree(s->dt);
     cudaFree(s->hist);
     cudaFree(s->partial);
     cudaFree(s->err);
-    cudaFree(s->staged);
     cudaFree(s->cfl_slot);
     if (s->own_stream) cudaStreamDestroy(s->own_stream);
     delete s;

@@ -18,6 +18,7 @@
 
 #include "dim_launch.h"
 #include "dimgpu.h"
+#include "range_alloc.h"
 
 using namespace dimgpu;
 
@@ -35,54 +36,6 @@ struct HostInst {
     int steps_left;       // host mirror (exact: every run advances min(n, left))
     long long cell_off;   // arena mode: first cell of its range (scratch items and state)
     long long dt_off;     // arena mode: first entry of its dt log range
-};
-
-// First-fit allocator of ranges of [0, capacity): the arena mode's cells and
-// dt-log entries.  Freed ranges merge with their neighbours.
-class RangeAlloc {
-public:
-    void reset(long long cap)
-    {
-        free_.clear();
-        if (cap > 0) free_[0] = cap;
-        used_ = 0;
-    }
-    long long alloc(long long n)
-    {
-        if (n <= 0) n = 1;
-        for (auto it = free_.begin(); it != free_.end(); ++it) {
-            if (it->second < n) continue;
-            const long long off = it->first, len = it->second;
-            free_.erase(it);
-            if (len > n) free_[off + n] = len - n;
-            used_ += n;
-            return off;
-        }
-        return -1;
-    }
-    void release(long long off, long long n)
-    {
-        if (n <= 0) n = 1;
-        used_ -= n;
-        auto it = free_.emplace(off, n).first;
-        auto nx = std::next(it);
-        if (nx != free_.end() && it->first + it->second == nx->first) {
-            it->second += nx->second;
-            free_.erase(nx);
-        }
-        if (it != free_.begin()) {
-            auto pv = std::prev(it);
-            if (pv->first + pv->second == it->first) {
-                pv->second += it->second;
-                free_.erase(it);
-            }
-        }
-    }
-    long long used() const { return used_; }
-
-private:
-    std::map<long long, long long> free_;
-    long long used_ = 0;
 };
 
 long long boundary_cells(const dimgpu_desc& d)
@@ -127,6 +80,7 @@ struct dimgpu_batch {
     RangeAlloc cells, dts;
     BInst* tab_pinned = nullptr;           // host staging of the tables
     long long* prefix_pinned = nullptr;    // cell prefix, then bc prefix
+    cudaEvent_t done = nullptr;            // after the last enqueued step
 };
 
 namespace {
@@ -328,6 +282,20 @@ void free_instance(dimgpu_batch* b, HostInst& h)
 
 }  // namespace
 
+namespace dimgpu {
+
+// 1 when every enqueued step has finished (dimgpu_batch_wait then returns
+// without blocking), 0 while steps run; no host synchronisation.
+int batch_ready(dimgpu_batch* b)
+{
+    if (!b->done) return 1;
+    const cudaError_t e = cudaEventQuery(b->done);
+    if (e == cudaErrorNotReady) return 0;
+    return 1;  // finished, or failed: dimgpu_batch_wait reports which
+}
+
+}  // namespace dimgpu
+
 extern "C" {
 
 int dimgpu_batch_create(int nmat, int dim, dimgpu_batch** out)
@@ -407,6 +375,7 @@ int dimgpu_batch_destroy(dimgpu_batch* b)
     if (!b) return DIMGPU_OK;
     if (b->stream) cudaStreamSynchronize(b->stream);
     drop_graphs(b);
+    if (b->done) cudaEventDestroy(b->done);
     if (!b->arena)
         for (auto& h : b->inst) free_instance(b, h);
     for (auto& p : b->st_arena) cudaFree(p);
@@ -576,6 +545,8 @@ int dimgpu_batch_enqueue(dimgpu_batch* b, int n)
             done += 1;
         }
     }
+    if (e == cudaSuccess && !b->done) e = cudaEventCreateWithFlags(&b->done, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(b->done, b->stream);
     if (e != cudaSuccess) return bcuda(b, e, "dimgpu_batch_enqueue");
     // host mirror: an instance with L steps left ran min(n, L) of them, and
     // ran in the last one iff L >= n
@@ -585,6 +556,7 @@ int dimgpu_batch_enqueue(dimgpu_batch* b, int n)
     }
     return DIMGPU_OK;
 }
+
 
 // Wait for every enqueued step; report a non-finite state or time step.
 int dimgpu_batch_wait(dimgpu_batch* b)

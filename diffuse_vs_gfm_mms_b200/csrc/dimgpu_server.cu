@@ -2,21 +2,30 @@
 // (include/dimgpu.h: dimgpu_server_*).
 //
 // Requests (a grid, its initial state, a step budget) are submitted from any
-// host thread and queue in arrival order.  A server thread runs the loop:
+// host thread and queue in arrival order.  A server thread drives two kinds
+// of lanes, each on its own CUDA stream:
 //
-//   admit    first come first served, per (material count, dimension) group,
-//            into that group's batch — an arena-mode dimgpu_batch whose
-//            device memory was reserved once, so admission allocates and
-//            synchronises nothing; a request that does not fit waits for
-//            room (later requests of other groups may go ahead);
-//   step     every group with resident solves enqueues one quantum of steps
-//            on its own stream, so the groups' work overlaps on the device;
-//   retire   after the quantum, finished solves are copied out and their
-//            arena ranges returned, which is what lets the queue drain.
+//   batch lanes  one per (material count, dimension) group: an arena-mode
+//                dimgpu_batch whose device memory was reserved once, holding
+//                the group's small solves;
+//   solo lanes   `solo_slots` session shells for solves of at least
+//                `solo_min_cells` cells, which fill the GPU on their own and
+//                run fastest as one grid (the staged single-grid sweep); their
+//                state and scratch are ranges of one solo arena, also
+//                reserved once.
+//
+// The loop never waits for all lanes together: a lane whose quantum (a few
+// steps, enqueued as one unit) has finished — found by an event query, no
+// host synchronisation — retires its finished solves, takes in queued ones
+// and gets its next quantum at once, while the other lanes keep running.
+// Admission is first come first served per lane kind and group and neither
+// allocates nor synchronises; a solve that does not fit waits for room
+// (later solves of other lanes may go ahead).
 //
 // Every solve's arithmetic is the single-grid step's: a result does not
-// depend on what else was resident.  Latency is measured on the host from
-// submission to the end of the quantum in which the solve finished.
+// depend on the lane or on what else was resident.  Latency is measured on
+// the host from submission to the completion of the quantum in which the
+// solve finished.
 #include <algorithm>
 #include <chrono>
 #include <condition_variable>
@@ -31,12 +40,16 @@
 
 #include "dim_launch.h"
 #include "dimgpu.h"
+#include "dimgpu_session.h"
+#include "range_alloc.h"
 
 using namespace dimgpu;
 
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+constexpr int kSoloHistCap = 4096;  // dt entries a session keeps between collections
 
 // Device bytes per cell of a resident solve in a group's arena: two state
 // copies and the staged-sweep scratch.
@@ -55,8 +68,9 @@ struct Req {
     double cfl = 0.0, dt_max = 0.0;
     int status = DIMGPU_REQ_QUEUED;
     bool cancel = false;
-    int group = -1;
-    int inst = -1;
+    int group = -1;   // batch lane
+    int inst = -1;    // instance in that lane's batch
+    int solo = -1;    // solo lane
     Clock::time_point submitted, finished;
     std::string msg;
 };
@@ -65,6 +79,16 @@ struct Group {
     int nmat = 0, dim = 0;
     dimgpu_batch* batch = nullptr;
     std::vector<long long> resident;  // request ids
+    bool busy = false;                // a quantum is in flight
+};
+
+struct Solo {
+    dimgpu_session* s = nullptr;
+    cudaEvent_t done = nullptr;
+    long long req = 0;                // resident request id, 0 when free
+    long long off = 0, len = 0;       // its range of the solo arena (doubles)
+    int steps_done = 0;               // steps enqueued so far
+    bool busy = false;
 };
 
 }  // namespace
@@ -79,6 +103,10 @@ struct dimgpu_server {
     std::deque<long long> queue;                      // queued request ids, arrival order
     std::map<long long, std::unique_ptr<Req>> reqs;   // every request not yet collected
     std::vector<Group> groups;
+    std::vector<Solo> solos;
+    double* solo_arena = nullptr;
+    RangeAlloc solo_cells;
+    std::string solo_error;                           // why the solo lanes could not be set up
     long long submitted = 0, completed = 0, cancelled = 0, failed = 0, quanta = 0;
     int resident = 0, peak_resident = 0;
     double peak_bytes = 0.0, used_bytes = 0.0;
@@ -92,6 +120,12 @@ int sfail(dimgpu_server* s, int code, const std::string& m)
     if (s) s->msg = m;
     set_sessionless_error(m);
     return code;
+}
+
+bool is_solo(const dimgpu_server* s, const dimgpu_desc& d, long long ncell)
+{
+    return s->cfg.solo_slots > 0 && s->cfg.solo_min_cells > 0 && ncell >= s->cfg.solo_min_cells &&
+           d.model == DIMGPU_MODEL_DIM;
 }
 
 // The group of a request, created (and its arena reserved) on first use.
@@ -122,6 +156,41 @@ int group_of(dimgpu_server* s, const dimgpu_desc& d, std::string* err)
     return (int)s->groups.size() - 1;
 }
 
+// The solo lanes and their arena, set up on first use.  Server thread only.
+bool solo_ready(dimgpu_server* s)
+{
+    if (!s->solos.empty()) return true;
+    if (!s->solo_error.empty()) return false;
+    const long long cap = (long long)(s->cfg.hbm_budget_bytes * s->cfg.solo_share / 8.0);
+    cudaError_t e = cap > 0 ? cudaMalloc(&s->solo_arena, sizeof(double) * (size_t)cap) : cudaErrorInvalidValue;
+    if (e != cudaSuccess) {
+        s->solo_error = std::string("reserving the solo arena: ") + cudaGetErrorString(e);
+        s->solo_arena = nullptr;
+        return false;
+    }
+    s->solo_cells.reset(cap);
+    for (int k = 0; k < s->cfg.solo_slots; ++k) {
+        Solo L;
+        int rc = session_shell_create(&L.s);
+        if (rc == DIMGPU_OK && cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming) != cudaSuccess)
+            rc = DIMGPU_E_CUDA;
+        if (rc != DIMGPU_OK) {
+            s->solo_error = std::string("creating the solo lanes: ") + dimgpu_last_error(nullptr);
+            if (L.s) dimgpu_destroy(L.s);
+            for (auto& o : s->solos) {
+                dimgpu_destroy(o.s);
+                cudaEventDestroy(o.done);
+            }
+            s->solos.clear();
+            cudaFree(s->solo_arena);
+            s->solo_arena = nullptr;
+            return false;
+        }
+        s->solos.push_back(L);
+    }
+    return true;
+}
+
 void finish(dimgpu_server* s, Req& r, int status, const std::string& msg = "")
 {
     r.status = status;
@@ -132,7 +201,7 @@ void finish(dimgpu_server* s, Req& r, int status, const std::string& msg = "")
     else if (status == DIMGPU_REQ_FAILED) s->failed++;
 }
 
-void release(dimgpu_server* s, Group& G, Req& r)
+void release_batch(dimgpu_server* s, Group& G, Req& r)
 {
     dimgpu_batch_remove(G.batch, r.inst);
     G.resident.erase(std::find(G.resident.begin(), G.resident.end(), r.id));
@@ -141,11 +210,42 @@ void release(dimgpu_server* s, Group& G, Req& r)
     r.inst = -1;
 }
 
-// Admission (lock held): first come first served within a group; a group
-// whose head does not fit admits nothing more this round.
+void release_solo(dimgpu_server* s, Solo& L, Req& r)
+{
+    s->solo_cells.release(L.off, L.len);
+    s->resident--;
+    s->used_bytes -= 8.0 * (double)L.len;
+    L.req = 0;
+    r.solo = -1;
+}
+
+void admitted(dimgpu_server* s, Req& r, double bytes)
+{
+    r.status = DIMGPU_REQ_RUNNING;
+    s->resident++;
+    s->peak_resident = std::max(s->peak_resident, s->resident);
+    s->used_bytes += bytes;
+    s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+}
+
+}  // namespace
+
+namespace {
+
+std::string session_message(const dimgpu_session* sess)
+{
+    const std::string m = dimgpu_last_error(sess);
+    return m.empty() ? std::string(dimgpu_last_error(nullptr)) : m;
+}
+
+// Admission (lock held): first come first served within the solo lanes and
+// within each batch group; a lane kind or group whose head cannot be taken
+// now (no free lane, no room, or its batch lane is mid-quantum) takes
+// nothing more this round, so its later requests cannot overtake it.
 void admit(dimgpu_server* s)
 {
     std::vector<char> blocked(s->groups.size() + 16, 0);
+    bool solo_blocked = false;
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         Req& r = *s->reqs[*it];
         if (r.cancel) {
@@ -160,6 +260,44 @@ void admit(dimgpu_server* s)
             continue;
         }
         if (s->resident >= s->cfg.max_slots) break;
+        if (is_solo(s, r.desc, r.ncell)) {
+            if (solo_blocked) {
+                ++it;
+                continue;
+            }
+            if (!solo_ready(s)) {
+                finish(s, r, DIMGPU_REQ_FAILED, s->solo_error);
+                it = s->queue.erase(it);
+                continue;
+            }
+            int lane = -1;
+            for (size_t k = 0; k < s->solos.size() && lane < 0; ++k)
+                if (s->solos[k].req == 0 && !s->solos[k].busy) lane = (int)k;
+            const long long need = session_grid_doubles(&r.desc);
+            const long long off = lane < 0 ? -1 : s->solo_cells.alloc(need);
+            if (off < 0) {
+                solo_blocked = true;
+                ++it;
+                continue;
+            }
+            Solo& L = s->solos[(size_t)lane];
+            int rc = session_shell_bind(L.s, &r.desc, s->solo_arena + off);
+            if (rc == DIMGPU_OK) rc = dimgpu_upload(L.s, r.state.data(), r.state.size());
+            if (rc != DIMGPU_OK) {
+                s->solo_cells.release(off, need);
+                finish(s, r, DIMGPU_REQ_FAILED, session_message(L.s));
+                it = s->queue.erase(it);
+                continue;
+            }
+            L.req = r.id;
+            L.off = off;
+            L.len = need;
+            L.steps_done = 0;
+            r.solo = lane;
+            admitted(s, r, 8.0 * (double)need);
+            it = s->queue.erase(it);
+            continue;
+        }
         std::string err;
         const int g = group_of(s, r.desc, &err);
         if (g < 0) {
@@ -168,11 +306,12 @@ void admit(dimgpu_server* s)
             continue;
         }
         if ((size_t)g >= blocked.size()) blocked.resize((size_t)g + 1, 0);
-        if (blocked[(size_t)g]) {
+        Group& G = s->groups[(size_t)g];
+        if (blocked[(size_t)g] || G.busy) {
+            blocked[(size_t)g] = 1;
             ++it;
             continue;
         }
-        Group& G = s->groups[(size_t)g];
         int iid = -1;
         const int rc = dimgpu_batch_add(G.batch, &r.desc, r.state.data(), r.steps, r.cfl, r.dt_max, &iid);
         if (rc == DIMGPU_E_OOM) {
@@ -187,77 +326,159 @@ void admit(dimgpu_server* s)
         }
         r.group = g;
         r.inst = iid;
-        r.status = DIMGPU_REQ_RUNNING;
         G.resident.push_back(r.id);
-        s->resident++;
-        s->peak_resident = std::max(s->peak_resident, s->resident);
-        s->used_bytes += bytes_per_cell(r.desc.nmat, r.desc.dim) * (double)r.ncell;
-        s->peak_bytes = std::max(s->peak_bytes, s->used_bytes);
+        admitted(s, r, bytes_per_cell(r.desc.nmat, r.desc.dim) * (double)r.ncell);
         it = s->queue.erase(it);
+    }
+}
+
+// A batch lane whose quantum has ended: copy out and retire its finished
+// solves (all of them, failed, on an error).
+void retire_batch(dimgpu_server* s, Group& G)
+{
+    G.busy = false;
+    const int rc = dimgpu_batch_wait(G.batch);  // the quantum has ended: returns at once
+    const std::string err = rc != DIMGPU_OK ? dimgpu_batch_last_error(G.batch) : "";
+    for (size_t q = 0; q < G.resident.size();) {
+        Req& r = *s->reqs[G.resident[q]];
+        int done = 0, left = 0;
+        dimgpu_batch_status(G.batch, r.inst, &done, &left);
+        if (rc == DIMGPU_OK && left > 0) {
+            ++q;
+            continue;
+        }
+        int st = DIMGPU_REQ_FAILED;
+        std::string m = err;
+        if (rc == DIMGPU_OK) {
+            r.dts.assign((size_t)std::max(done, 1), 0.0);
+            const int rd = dimgpu_batch_download(G.batch, r.inst, r.state.data(), r.state.size(), r.dts.data());
+            r.dts.resize((size_t)done);
+            st = rd == DIMGPU_OK ? DIMGPU_REQ_DONE : DIMGPU_REQ_FAILED;
+            if (rd != DIMGPU_OK) m = dimgpu_batch_last_error(G.batch);
+        }
+        release_batch(s, G, r);
+        finish(s, r, st, m);
+    }
+}
+
+// A solo lane whose quantum has ended: check its error flag; when every step
+// has run, collect the dt log and the state.
+void retire_solo(dimgpu_server* s, Solo& L)
+{
+    L.busy = false;
+    Req& r = *s->reqs[L.req];
+    int rc = session_check(L.s);
+    if (rc == DIMGPU_OK && L.steps_done < r.steps) return;
+    if (rc == DIMGPU_OK) {
+        r.dts.assign((size_t)r.steps, 0.0);
+        int count = 0;
+        rc = dimgpu_collect(L.s, r.dts.data(), r.steps, &count);
+        if (rc == DIMGPU_OK) rc = dimgpu_download(L.s, r.state.data(), r.state.size());
+        r.dts.resize((size_t)count);
+    }
+    const std::string m = rc == DIMGPU_OK ? "" : session_message(L.s);
+    release_solo(s, L, r);
+    finish(s, r, rc == DIMGPU_OK ? DIMGPU_REQ_DONE : DIMGPU_REQ_FAILED, m);
+}
+
+// Cancellations of resident solves, on lanes between quanta.
+void cancel_resident(dimgpu_server* s)
+{
+    for (auto& G : s->groups) {
+        if (G.busy) continue;
+        for (size_t k = 0; k < G.resident.size();) {
+            Req& r = *s->reqs[G.resident[k]];
+            if (!r.cancel) {
+                ++k;
+                continue;
+            }
+            release_batch(s, G, r);
+            finish(s, r, DIMGPU_REQ_CANCELLED);
+        }
+    }
+    for (auto& L : s->solos) {
+        if (L.busy || L.req == 0) continue;
+        Req& r = *s->reqs[L.req];
+        if (!r.cancel) continue;
+        release_solo(s, L, r);
+        finish(s, r, DIMGPU_REQ_CANCELLED);
+    }
+}
+
+// The next quantum on every idle lane that holds solves.
+void enqueue_lanes(dimgpu_server* s)
+{
+    for (auto& G : s->groups) {
+        if (G.busy || G.resident.empty()) continue;
+        if (dimgpu_batch_enqueue(G.batch, s->cfg.quantum) == DIMGPU_OK) {
+            G.busy = true;
+            s->quanta++;
+            continue;
+        }
+        const std::string err = dimgpu_batch_last_error(G.batch);
+        while (!G.resident.empty()) {
+            Req& r = *s->reqs[G.resident.back()];
+            release_batch(s, G, r);
+            finish(s, r, DIMGPU_REQ_FAILED, err);
+        }
+    }
+    for (auto& L : s->solos) {
+        if (L.busy || L.req == 0) continue;
+        Req& r = *s->reqs[L.req];
+        const int n = std::min(s->cfg.quantum, r.steps - L.steps_done);
+        int rc = dimgpu_enqueue_steps(L.s, n, r.cfl, r.dt_max);
+        if (rc == DIMGPU_OK && cudaEventRecord(L.done, L.s->stream) != cudaSuccess) rc = DIMGPU_E_CUDA;
+        if (rc == DIMGPU_OK) {
+            L.steps_done += n;
+            L.busy = true;
+            s->quanta++;
+            continue;
+        }
+        const std::string m = session_message(L.s);
+        release_solo(s, L, r);
+        finish(s, r, DIMGPU_REQ_FAILED, m);
     }
 }
 
 void serve_loop(dimgpu_server* s)
 {
     std::unique_lock<std::mutex> lock(s->mu);
-    while (true) {
-        s->cv.wait(lock, [&] { return s->stop || !s->queue.empty() || s->resident > 0; });
-        if (s->stop) break;
-        // cancellations of resident solves
-        for (auto& G : s->groups) {
-            for (size_t k = 0; k < G.resident.size();) {
-                Req& r = *s->reqs[G.resident[k]];
-                if (r.cancel) {
-                    release(s, G, r);
-                    finish(s, r, DIMGPU_REQ_CANCELLED);
-                }
-                else {
-                    ++k;
-                }
+    while (!s->stop) {
+        bool progressed = false;
+        for (auto& G : s->groups)
+            if (G.busy && batch_ready(G.batch)) {
+                retire_batch(s, G);
+                progressed = true;
             }
-        }
+        for (auto& L : s->solos)
+            if (L.busy && cudaEventQuery(L.done) != cudaErrorNotReady) {
+                retire_solo(s, L);
+                progressed = true;
+            }
+        cancel_resident(s);
         admit(s);
-        if (s->resident == 0) {
-            s->cv.notify_all();
+        enqueue_lanes(s);
+        bool busy = false;
+        for (auto& G : s->groups) busy = busy || G.busy;
+        for (auto& L : s->solos) busy = busy || L.busy;
+        if (progressed || !busy) s->cv.notify_all();
+        if (busy) {
+            if (!progressed) {
+                // lanes are mid-quantum: look again shortly (no host sync)
+                lock.unlock();
+                std::this_thread::sleep_for(std::chrono::microseconds(50));
+                lock.lock();
+            }
             continue;
         }
-        // one quantum on every group, each on its own stream, then wait for all
-        std::vector<int> ran;
-        for (size_t g = 0; g < s->groups.size(); ++g) {
-            if (s->groups[g].resident.empty()) continue;
-            if (dimgpu_batch_enqueue(s->groups[g].batch, s->cfg.quantum) == DIMGPU_OK) ran.push_back((int)g);
+        if (s->resident == 0 && !s->queue.empty()) {
+            // nothing runs and the head still was not taken: it never fits
+            Req& r = *s->reqs[s->queue.front()];
+            finish(s, r, DIMGPU_REQ_FAILED, "the solve cannot be admitted within the server's limits");
+            s->queue.pop_front();
+            continue;
         }
-        lock.unlock();
-        std::vector<int> rcs(ran.size());
-        for (size_t k = 0; k < ran.size(); ++k) rcs[k] = dimgpu_batch_wait(s->groups[(size_t)ran[k]].batch);
-        lock.lock();
-        s->quanta++;
-        // retire finished solves (and fail the group's solves on an error)
-        for (size_t k = 0; k < ran.size(); ++k) {
-            Group& G = s->groups[(size_t)ran[k]];
-            const std::string err = rcs[k] != DIMGPU_OK ? dimgpu_batch_last_error(G.batch) : "";
-            for (size_t q = 0; q < G.resident.size();) {
-                Req& r = *s->reqs[G.resident[q]];
-                int done = 0, left = 0;
-                dimgpu_batch_status(G.batch, r.inst, &done, &left);
-                if (rcs[k] == DIMGPU_OK && left > 0) {
-                    ++q;
-                    continue;
-                }
-                int st = DIMGPU_REQ_FAILED;
-                std::string m = err;
-                if (rcs[k] == DIMGPU_OK) {
-                    r.dts.assign((size_t)std::max(done, 1), 0.0);
-                    const int rc = dimgpu_batch_download(G.batch, r.inst, r.state.data(), r.state.size(), r.dts.data());
-                    r.dts.resize((size_t)done);
-                    st = rc == DIMGPU_OK ? DIMGPU_REQ_DONE : DIMGPU_REQ_FAILED;
-                    if (rc != DIMGPU_OK) m = dimgpu_batch_last_error(G.batch);
-                }
-                release(s, G, r);
-                finish(s, r, st, m);
-            }
-        }
-        s->cv.notify_all();
+        s->cv.wait(lock, [&] { return s->stop || !s->queue.empty(); });
     }
 }
 
@@ -272,13 +493,18 @@ int dimgpu_server_create(const dimgpu_server_config* cfg, dimgpu_server** out)
     if (!(cfg->hbm_budget_bytes > 0.0) || cfg->max_slots < 1 || cfg->quantum < 1 || cfg->max_steps_per_solve < 1)
         return sfail(nullptr, DIMGPU_E_INVALID_ARG,
                      "dimgpu_server_create: budget, slots, quantum and steps per solve must be positive");
-    double sum = 0.0;
+    double sum = cfg->solo_share;
+    if (!(cfg->solo_share >= 0.0) || cfg->solo_slots < 0 || cfg->solo_min_cells < 0)
+        return sfail(nullptr, DIMGPU_E_INVALID_ARG, "dimgpu_server_create: negative solo setting");
     for (double f : cfg->dim_share) {
         if (!(f >= 0.0)) return sfail(nullptr, DIMGPU_E_INVALID_ARG, "dimgpu_server_create: negative budget share");
         sum += f;
     }
     if (!(sum > 0.0) || sum > 1.0 + 1e-12)
         return sfail(nullptr, DIMGPU_E_INVALID_ARG, "dimgpu_server_create: budget shares must add up to (0, 1]");
+    if (cfg->solo_slots > 0 && cfg->solo_min_cells > 0 && cfg->max_steps_per_solve > kSoloHistCap)
+        return sfail(nullptr, DIMGPU_E_INVALID_ARG,
+                     "dimgpu_server_create: solo lanes keep at most 4096 steps per solve");
     auto* s = new dimgpu_server();
     s->cfg = *cfg;
     s->worker = std::thread(serve_loop, s);
@@ -296,6 +522,11 @@ int dimgpu_server_destroy(dimgpu_server* s)
     s->cv.notify_all();
     if (s->worker.joinable()) s->worker.join();
     for (auto& G : s->groups) dimgpu_batch_destroy(G.batch);
+    for (auto& L : s->solos) {
+        dimgpu_destroy(L.s);
+        cudaEventDestroy(L.done);
+    }
+    cudaFree(s->solo_arena);
     delete s;
     return DIMGPU_OK;
 }
@@ -316,8 +547,11 @@ int dimgpu_server_submit(dimgpu_server* s, const dimgpu_desc* desc, const double
         ncell *= desc->N[a];
         if (ncell > (1LL << 40)) return sfail(s, DIMGPU_E_OOM, "dimgpu_server_submit: grid too large");
     }
-    const double need = bytes_per_cell(desc->nmat, desc->dim) * (double)ncell;
-    if (need > s->cfg.hbm_budget_bytes * s->cfg.dim_share[desc->dim - 1])
+    const bool solo = is_solo(s, *desc, ncell);
+    const double need = solo ? 8.0 * (double)session_grid_doubles(desc)
+                             : bytes_per_cell(desc->nmat, desc->dim) * (double)ncell;
+    const double share = solo ? s->cfg.solo_share : s->cfg.dim_share[desc->dim - 1];
+    if (need > s->cfg.hbm_budget_bytes * share)
         return sfail(s, DIMGPU_E_OOM, "dimgpu_server_submit: the solve needs more device memory than its budget share");
     auto r = std::make_unique<Req>();
     r->desc = *desc;

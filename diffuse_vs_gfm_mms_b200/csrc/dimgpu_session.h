@@ -39,6 +39,7 @@ struct dimgpu_session {
     std::vector<cudaEvent_t> pool;
     double prof[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     int pending = 0;  // steps enqueued since the last collection
+    bool borrowed = false;  // buf[] and staged point into a caller's arena (a shell)
 };
 
 namespace dimgpu {
@@ -60,5 +61,14 @@ cudaError_t session_sweep(dimgpu_session* s, int dir);
 cudaError_t session_bc(dimgpu_session* s);
 // Waits for the session's stream and turns its error flag into a status.
 int session_check(dimgpu_session* s);
+
+// Session shells (the serving loop's solo slots): a session with its stream
+// and small device buffers but no grid memory; binding gives it a grid whose
+// state buffers and staged scratch are a caller-owned device range of
+// session_grid_doubles(desc) doubles, so a request is admitted without an
+// allocation or a synchronisation.  Binding validates the descriptor.
+long long session_grid_doubles(const dimgpu_desc* desc);
+int session_shell_create(dimgpu_session** out);
+int session_shell_bind(dimgpu_session* s, const dimgpu_desc* desc, double* mem);
 
 }  // namespace dimgpu

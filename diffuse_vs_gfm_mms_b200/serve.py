@@ -89,7 +89,8 @@ class Server:
     requests at their arrival times and collects the results."""
 
     def __init__(self, hbm_budget_bytes: float = 150e9, max_slots: int = 128, quantum: int = 8,
-                 dim_share=(0.4, 0.6, 0.0), max_steps_per_solve: int = 4096):
+                 dim_share=(0.1, 0.4, 0.0), max_steps_per_solve: int = 4096, solo_min_cells: int = 1 << 18,
+                 solo_share: float = 0.5, solo_slots: int = 4):
         cfg = abi.ServerConfig()
         cfg.hbm_budget_bytes = float(hbm_budget_bytes)
         for k in range(3):
@@ -97,6 +98,9 @@ class Server:
         cfg.max_slots = max_slots
         cfg.quantum = quantum
         cfg.max_steps_per_solve = max_steps_per_solve
+        cfg.solo_min_cells = solo_min_cells
+        cfg.solo_share = float(solo_share)
+        cfg.solo_slots = solo_slots
         h = C.c_void_p()
         self._check(lib().dimgpu_server_create(C.byref(cfg), C.byref(h)), None)
         self._h = h

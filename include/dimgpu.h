@@ -367,13 +367,17 @@ int dimgpu_slabs_download(dimgpu_slabs* L, double* soa, size_t count);
  * Continuous batching of DIM solve requests.  No counterpart in the
  * reference, which runs one case per process (run_dim_case,
  * src/app/solver/run_dim.hpp:20-178).  Requests are submitted from any host
- * thread and queue in arrival order; a server thread admits them first come
- * first served (per material count and dimension) into batches whose device
- * memory was reserved once from the budget (dimgpu_batch_reserve), so
- * admission allocates and synchronises nothing; every quantum it advances
- * all resident solves, each group on its own stream so the groups overlap
- * on the device, and retires the finished ones, which frees their room for
- * the queue.  A result is exactly the single-grid step's. */
+ * thread and queue in arrival order.  A server thread drives lanes, each on
+ * its own stream: batch lanes (one per material count and dimension, an
+ * arena batch reserved once from the budget, dimgpu_batch_reserve) for
+ * small solves, and solo lanes (session shells over one reserved arena) for
+ * solves of at least solo_min_cells cells, which fill the GPU alone and run
+ * fastest as one grid.  Admission is first come first served per lane kind
+ * and group and allocates and synchronises nothing.  Each lane advances its
+ * solves a quantum at a time; when a lane's quantum ends (an event query)
+ * it retires its finished solves, takes queued ones and starts its next
+ * quantum while the other lanes run on.  A result is exactly the single-grid
+ * step's. */
 typedef struct dimgpu_server dimgpu_server;
 
 typedef struct dimgpu_server_config {
@@ -382,6 +386,9 @@ typedef struct dimgpu_server_config {
     int max_slots;             /* resident solves at most */
     int quantum;               /* steps per scheduling round */
     int max_steps_per_solve;   /* largest step budget a request may ask for */
+    long long solo_min_cells;  /* solves of at least this many cells run alone on a solo lane (0: never) */
+    double solo_share;         /* fraction of the budget for solo solves (sum with dim_share <= 1) */
+    int solo_slots;            /* solo lanes (solves resident alone at once); 0: none */
 } dimgpu_server_config;
 
 enum {

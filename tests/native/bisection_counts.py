@@ -25,7 +25,7 @@ from diffuse_vs_gfm_mms_b200 import workloads as W  # noqa: E402
 from diffuse_vs_gfm_mms_b200.abi import dptr  # noqa: E402
 
 NAMES = ["recoveries", "doublings", "certain_steps", "literal_evals", "no_bracket", "repairs",
-         "repair_recoveries", "repair_floors", "sound_speeds"]
+         "repair_recoveries", "repair_floors", "sound_speeds", "doublings_skipped"]
 
 
 def counts(lib, d, U, dt):
@@ -46,7 +46,7 @@ def table(title, samples):
     print(f"{'step':>5} {'axis':>4} " + " ".join(f"{n:>17}" for n in NAMES) + f" {'iters/recovery':>15}")
     for step, rows in samples:
         for axis, r in enumerate(rows):
-            iters = (r[1] + r[2] + r[3]) / max(r[0], 1e-30)
+            iters = (r[1] + r[2] + r[3] + r[9]) / max(r[0], 1e-30)
             print(f"{step:5d} {'xyz'[axis]:>4} " + " ".join(f"{v:17.3f}" for v in r) + f" {iters:15.2f}")
 
 

@@ -10,6 +10,7 @@
 // Operation counts (dimgpu::OpCount) of everything this harness runs.
 static long long g_opcount[16];
 #define DIMGPU_OPCOUNT(k) (++g_opcount[(k)])
+#define DIMGPU_OPCOUNT_ADD(k, n) (g_opcount[(k)] += (n))
 
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_line.h"
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_mixed.h"
