@@ -602,7 +602,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double
 // faces): reconstruct, build, repair, flux -> the LS / RS slots.  Each
 // routine has one call site here, so all are inlined.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bf(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_bf(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                  StagedBufs<NM, D> b)
 {
     const long long N = (long long)ls.nl * ls.n;
@@ -661,7 +661,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const doubl
 // Stage C: one thread per face state (left faces first, then right faces),
 // all routines inlined.  End cells keep U and its primitive on both sides.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_c(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_c(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b)
 {
     const long long N = (long long)ls.nl * ls.n;

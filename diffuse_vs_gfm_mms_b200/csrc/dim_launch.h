@@ -21,10 +21,16 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_MINB 3
 #endif
 
+// Resident blocks per SM of the per-face-state kernels (staged_bf, staged_c).
+#ifndef DIMGPU_FACE_MINB
+#define DIMGPU_FACE_MINB DIMGPU_STAGED_MINB
+#endif
+
 // Whether the staged D and E kernels inline their sound speeds and repairs
 // (two call sites each) instead of calling the out-of-line copies.
+// Measured on a B200: 1.5 % less time per step on c1 and c2 inlined.
 #ifndef DIMGPU_STAGED_INLINE_DE
-#define DIMGPU_STAGED_INLINE_DE false
+#define DIMGPU_STAGED_INLINE_DE true
 #endif
 
 namespace dimgpu {

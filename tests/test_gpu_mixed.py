@@ -202,3 +202,34 @@ def test_fp32_cost_against_the_fp64_twin(port, name, gen, cfl, n):
     assert np.all(np.isfinite(out)) and np.all(np.isfinite(twin))
     bound = REL_L1_TOL if sens.max() <= 1e-7 else max(REL_L1_TOL, 10.0 * sens.max())
     assert np.all(fp32 <= bound), (fp32, sens)
+
+
+def test_fp32_cost_at_full_size_after_the_interaction():
+    """c1 at its full 1024x512 through the shock-bubble interaction (400
+    steps; the shock reaches the bubble after about 230): mixed against its
+    FP64 twin on the whole field, with the twin's own 1e-15-perturbation
+    response as the conditioning bound, and the twin against the reference's
+    own 400-step record (tests/golden/long_c1_shock_bubble_1024x512.npz,
+    sampled cells) for what the algorithm's shortcuts cost."""
+    import os
+
+    from helpers import GOLDEN
+
+    d, U = W.shock_bubble_2d(N=(1024, 512))
+    n = 400
+    out, dts = _mixed(d, U, 0.8, n)
+    twin, tdts = _twin(d, U, 0.8, n)
+    rng = np.random.default_rng(11)
+    tp, _ = _twin(d, U * (1.0 + 1e-15 * rng.standard_normal(U.shape)), 0.8, n)
+    fp32 = _report("c1 2D shock-bubble 1024x512, 400 steps — mixed vs FP64 twin", out, twin, dts, tdts, d)
+    sens = _rel_l1_scored(tp, twin, d)
+    print(f"  twin moved by a 1e-15 input perturbation: rel L1 {_fmt(sens)}")
+    path = os.path.join(GOLDEN, "long_c1_shock_bubble_1024x512.npz")
+    if os.path.exists(path):
+        rec = np.load(path)
+        idx = rec["sample_index"]
+        _report("c1 1024x512, 400 steps — FP64 twin vs the reference (sampled cells)", twin[:, idx],
+                rec[f"s{n}_sample"], tdts, rec["dt"][:n], d)
+    assert np.all(np.isfinite(out)) and np.all(np.isfinite(twin))
+    bound = REL_L1_TOL if sens.max() <= 1e-7 else max(REL_L1_TOL, 10.0 * sens.max())
+    assert np.all(fp32 <= bound), (fp32, sens)
