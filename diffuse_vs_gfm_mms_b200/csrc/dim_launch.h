@@ -21,9 +21,11 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_MINB 3
 #endif
 
-// Resident blocks per SM of the per-face-state kernels (staged_bf, staged_c).
+// Resident blocks per SM of the per-face-state kernels (staged_bf, staged_c),
+// whose threads carry one face state each: 64 registers.  Measured on a
+// B200: 3.5 % less time per step on c2 (512^3) than at 3 blocks, 0.3 % on c1.
 #ifndef DIMGPU_FACE_MINB
-#define DIMGPU_FACE_MINB DIMGPU_STAGED_MINB
+#define DIMGPU_FACE_MINB 4
 #endif
 
 // Whether the staged D and E kernels inline their sound speeds and repairs
