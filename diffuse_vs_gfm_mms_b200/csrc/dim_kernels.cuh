@@ -753,12 +753,12 @@ __global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, __
         State<NM, D> U;
         load_cell<NM, D>(in, g.ncell, it.cell, U);
         CellA<NM, D> A;
-        stage_a_mixed<NM, D>(M, U, A);
+        stage_a_mixed<NM, D, DIMGPU_MIXED_INLINE>(M, U, A);
         g_put<NM, D>(b.P, b.cap, t, A.P);
         g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
-        if (fc.on) best = cfl_candidate<NM, D>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+        if (fc.on) best = cfl_candidate<NM, D, DIMGPU_MIXED_INLINE>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
     }
     if (fc.on) fused_cfl_reduce(best, fc);
 }
@@ -791,7 +791,7 @@ __global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in,
         Prim<NM, D> lo, hi;
         g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
         g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
-        stage_b_mixed<NM, D, R>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
+        stage_b_mixed<NM, D, R, DIMGPU_MIXED_INLINE>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
     }
     g_put<NM, D>(b.Ph, b.cap, t, Ph);
 }
@@ -812,7 +812,7 @@ __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const 
     g_get<NM, D>(b.Ph, b.cap, t - it.s, lo);
     g_get<NM, D>(b.Ph, b.cap, t, c);
     g_get<NM, D>(b.Ph, b.cap, t + it.s, hi);
-    face_mixed<NM, D, R>(M, lo, c, hi, right, Uf, Pf);
+    face_mixed<NM, D, R, DIMGPU_MIXED_INLINE>(M, lo, c, hi, right, Uf, Pf);
 }
 
 template<int NM, int D, int DIR, typename R = float>
@@ -832,7 +832,7 @@ __global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in
     nx.cell += g.stride[DIR];
     mixed_face<NM, D, DIR, R>(in, g, M, b, nx, t + it.s, n, false, UR, PR);
     FaceD<NM, D> f;
-    if (!stage_d_mixed<NM, D, R>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+    if (!stage_d_mixed<NM, D, R, DIMGPU_MIXED_INLINE>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
     g_put<NM, D>(b.F, b.cap, t, f);
 }
 

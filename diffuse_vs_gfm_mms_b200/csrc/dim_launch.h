@@ -28,6 +28,12 @@ struct dimgpu_batch;
 #define DIMGPU_FACE_MINB 4
 #endif
 
+// Whether the mixed-precision kernels (mixed_a, mixed_b, mixed_cd) inline
+// their recoveries, conversions, repairs and sound speeds.
+#ifndef DIMGPU_MIXED_INLINE
+#define DIMGPU_MIXED_INLINE false
+#endif
+
 // Whether the staged D and E kernels inline their sound speeds and repairs
 // (two call sites each) instead of calling the out-of-line copies.
 // Measured on a B200: 1.5 % less time per step on c1 and c2 inlined.

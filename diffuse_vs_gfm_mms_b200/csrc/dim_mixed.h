@@ -123,7 +123,7 @@ DHD double pressure_closed_form(const Mats& M, double rho_total, double e, const
 
 // cons_to_prim (primitives.hpp:111-162) with the closed-form recovery.
 template<int NM, int D>
-DNI Prim<NM, D> cons_to_prim_mixed_v(const Mats& M, State<NM, D> U)
+DHD Prim<NM, D> cons_to_prim_mixed_t(const Mats& M, State<NM, D> U)
 {
     Prim<NM, D> P;
     full_alpha<NM, D>(U, P.alpha);
@@ -150,16 +150,30 @@ DNI Prim<NM, D> cons_to_prim_mixed_v(const Mats& M, State<NM, D> U)
 }
 
 template<int NM, int D>
+DNI Prim<NM, D> cons_to_prim_mixed_v(const Mats& M, State<NM, D> U)
+{
+    return cons_to_prim_mixed_t<NM, D>(M, U);
+}
+
+template<int NM, int D>
 DHD void cons_to_prim_mixed(const Mats& M, const State<NM, D>& U, Prim<NM, D>& P)
 {
     P = cons_to_prim_mixed_v<NM, D>(M, U);
 }
 
+// The mixed recovery inlined (IL, kernels with one call site) or out of line.
+template<int NM, int D, bool IL>
+DHD Prim<NM, D> c2p_mixed(const Mats& M, const State<NM, D>& U)
+{
+    if constexpr (IL) return cons_to_prim_mixed_t<NM, D>(M, U);
+    else return cons_to_prim_mixed_v<NM, D>(M, U);
+}
+
 // Stage A of the mixed step (stage_a with the closed-form recovery).
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD void stage_a_mixed(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 {
-    cons_to_prim_mixed<NM, D>(M, U, A.P);
+    A.P = c2p_mixed<NM, D, IL>(M, U);
     A.Pe = A.P;
     enforce_positive_primitive<NM, D>(A.Pe);
     rhs_sound_speeds<NM, D>(M, A.P, A.ck);
@@ -179,7 +193,7 @@ DHD void stage_a_mixed(const Mats& M, const State<NM, D>& U, CellA<NM, D>& A)
 // rounding of the increments only.  For mirror states at a wall
 // (p_L = p_R, a_L = -a_R, u_L = -u_R) a_R / (a_L - a_R) is exactly -1/2, s*
 // is exactly 0, and so are the mass and energy fluxes.
-template<int NM, int D, typename R = float>
+template<int NM, int D, typename R = float, bool IL = false>
 DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& UR, const Prim<NM, D>& PL,
                     const Prim<NM, D>& PR, int dir, Flux<NM, D>& F, double& s_face)
 {
@@ -191,8 +205,8 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
     if (pL <= 0.0) pL = 1e-10;
     if (pR <= 0.0) pR = 1e-10;
     const double unL = PL.vel[dir], unR = PR.vel[dir];
-    const double cL = generic_mixture_sound_speed<NM>(M, rhoL, pL, PL.alpha, PL.rho);
-    const double cR = generic_mixture_sound_speed<NM>(M, rhoR, pR, PR.alpha, PR.rho);
+    const double cL = sound<NM, IL>(M, rhoL, pL, PL.alpha, PL.rho);
+    const double cR = sound<NM, IL>(M, rhoR, pR, PR.alpha, PR.rho);
     const double sL = dmin(unL - cL, unR - cR);
     const double sR = dmax(unL + cL, unR + cR);
 
@@ -258,7 +272,7 @@ DHD bool hllc_mixed(const Mats& M, const State<NM, D>& UL, const State<NM, D>& U
 // repair round trip, FP64 Hancock half step (hancock_predict's arithmetic,
 // muscl.hpp:143-191, evaluated face by face as in stage_b) and FP64
 // recovery into Ph.
-template<int NM, int D, typename R = float>
+template<int NM, int D, typename R = float, bool IL = false>
 DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
                        const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, Prim<NM, D>& Ph)
 {
@@ -272,13 +286,11 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
     reconstruct_mixed<NM, D, R>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
     Flux<NM, D> FL, FR;
     {
-        State<NM, D> Ul;
-        prim_to_cons<NM, D>(M, Pl, Ul);
+        const State<NM, D> Ul = p2c<NM, D, IL>(M, Pl);
         flux_normal<NM, D>(Ul, Pl, dir, FL);
     }
     {
-        State<NM, D> Ur;
-        prim_to_cons<NM, D>(M, Pr, Ur);
+        const State<NM, D> Ur = p2c<NM, D, IL>(M, Pr);
         flux_normal<NM, D>(Ur, Pr, dir, FR);
     }
     const double factor = 0.5 * dt / dx;
@@ -301,8 +313,8 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
     sanitise_alpha<NM>(alpha_new, 0.0);
 #pragma unroll
     for (int k = 0; k < NM - 1; ++k) Uh.a[k] = alpha_new[k];
-    repair_state<NM, D>(M, Uh);
-    cons_to_prim_mixed<NM, D>(M, Uh, Ph);
+    Uh = repair<NM, D, IL>(M, Uh);
+    Ph = c2p_mixed<NM, D, IL>(M, Uh);
     enforce_positive_primitive<NM, D>(Ph);
 }
 
@@ -310,7 +322,7 @@ DHD void stage_b_mixed(const Mats& M, const State<NM, D>& U, const CellA<NM, D>&
 // left) face of a cell from the half-step primitives of the cell and its
 // neighbours (reconstruct_mixed, one side only).  An end cell's face state
 // is its own state U and primitive P instead (as in stage_c).
-template<int NM, int D, typename R = float>
+template<int NM, int D, typename R = float, bool IL = false>
 DHD void face_mixed(const Mats& M, const Prim<NM, D>& Ph_lo, const Prim<NM, D>& Ph, const Prim<NM, D>& Ph_hi,
                     bool right, State<NM, D>& Uf, Prim<NM, D>& Pf)
 {
@@ -324,15 +336,15 @@ DHD void face_mixed(const Mats& M, const Prim<NM, D>& Ph_lo, const Prim<NM, D>& 
     for (int d = 0; d < D; ++d) Pf.vel[d] = Ph.vel[d] + sg * half_slope_mixed<R>(Ph_lo.vel[d], Ph.vel[d], Ph_hi.vel[d]);
     Pf.p = Ph.p + sg * half_slope_mixed<R>(Ph_lo.p, Ph.p, Ph_hi.p);
     enforce_positive_primitive<NM, D>(Pf);
-    prim_to_cons<NM, D>(M, Pf, Uf);
+    Uf = p2c<NM, D, IL>(M, Pf);
 }
 
 // Stage D of the mixed step: HLLC at face i|i+1 and the upwind alpha flux.
-template<int NM, int D, typename R = float>
+template<int NM, int D, typename R = float, bool IL = false>
 DHD bool stage_d_mixed(const Mats& M, const State<NM, D>& UL, const Prim<NM, D>& PL, const State<NM, D>& UR,
                        const Prim<NM, D>& PR, int dir, FaceD<NM, D>& out)
 {
-    const bool ok = hllc_mixed<NM, D, R>(M, UL, UR, PL, PR, dir, out.F, out.fv);
+    const bool ok = hllc_mixed<NM, D, R, IL>(M, UL, UR, PL, PR, dir, out.F, out.fv);
     const double* up = (out.fv >= 0.0) ? PL.alpha : PR.alpha;
 #pragma unroll
     for (int k = 0; k < NM; ++k) out.af[k] = up[k] * out.fv;
