@@ -139,7 +139,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_a(const BInst* 
     load_cell<NM, D>(in, I.g.ncell, it.cell, U);
     CellA<NM, D> A;
     if (I.mixed) stage_a_mixed<NM, D>(I.M, U, A);
-    else stage_a<NM, D>(I.M, U, A);
+    else stage_a<NM, D, DIMGPU_BATCH_INLINE>(I.M, U, A);
     g_put<NM, D>(b.P, b.cap, q, A.P);
     g_put<NM, D>(b.Pe, b.cap, q, A.Pe);
 #pragma unroll
@@ -173,7 +173,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_b(const BInst* 
         }
         else {
             State<NM, D> Uh;
-            stage_b<NM, D>(I.M, U, A, lo, hi, false, DIR, I.dt, I.g.dx[DIR], Uh, Ph);
+            stage_b<NM, D, DIMGPU_BATCH_INLINE>(I.M, U, A, lo, hi, false, DIR, I.dt, I.g.dx[DIR], Uh, Ph);
         }
     }
     g_put<NM, D>(b.Ph, b.cap, q, Ph);
@@ -202,7 +202,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_c(const BInst* 
         g_get<NM, D>(b.Ph, b.cap, q, Ph);
         g_get<NM, D>(b.Ph, b.cap, q - it.s, lo);
         g_get<NM, D>(b.Ph, b.cap, q + it.s, hi);
-        stage_c<NM, D>(I.M, U, A, Ph, lo, hi, false, LS, RS, PLS, PRS);
+        stage_c<NM, D, DIMGPU_BATCH_INLINE>(I.M, U, A, Ph, lo, hi, false, LS, RS, PLS, PRS);
     }
     g_put<NM, D>(b.LS, b.cap, q, LS);
     g_put<NM, D>(b.RS, b.cap, q, RS);
@@ -234,7 +234,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_d(const BInst* 
         g_get<NM, D>(b.PRS, b.cap, q, PL);
         g_get<NM, D>(b.LS, b.cap, q + it.s, UR);
         g_get<NM, D>(b.PLS, b.cap, q + it.s, PR);
-        if (!stage_d<NM, D>(I.M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+        if (!stage_d<NM, D, DIMGPU_BATCH_INLINE>(I.M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
     }
     g_put<NM, D>(b.F, b.cap, q, f);
     BATCH_LOOP_END
@@ -264,7 +264,8 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_e(const BInst* 
     if (!first) g_get<NM, D>(b.F, b.cap, q - it.s, lo);
     if (!last) g_get<NM, D>(b.F, b.cap, q, hi);
     State<NM, D> Un;
-    stage_e<NM, D>(I.M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, I.dt, I.g.dx[DIR], Un);
+    stage_e<NM, D, DIMGPU_BATCH_INLINE>(I.M, U, A, first ? nullptr : &lo, last ? nullptr : &hi, first, last, I.dt,
+                                         I.g.dx[DIR], Un);
     store_cell<NM, D>(out, I.g.ncell, it.cell, Un);
     BATCH_LOOP_END
 }

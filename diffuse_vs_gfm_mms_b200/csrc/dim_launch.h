@@ -29,9 +29,16 @@ struct dimgpu_batch;
 #endif
 
 // Whether the mixed-precision kernels (mixed_a, mixed_b, mixed_cd) inline
-// their recoveries, conversions, repairs and sound speeds.
+// their recoveries, conversions, repairs and sound speeds.  Measured on a
+// B200: 2 % less time per step on c1, 3 % on c2 (512^3) inlined.
 #ifndef DIMGPU_MIXED_INLINE
-#define DIMGPU_MIXED_INLINE false
+#define DIMGPU_MIXED_INLINE true
+#endif
+
+// Whether the batch kernels inline the FP64 stages' routines (the mixed
+// instances of a batch always call the out-of-line copies).
+#ifndef DIMGPU_BATCH_INLINE
+#define DIMGPU_BATCH_INLINE false
 #endif
 
 // Whether the staged D and E kernels inline their sound speeds and repairs

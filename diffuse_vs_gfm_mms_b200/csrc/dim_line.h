@@ -126,7 +126,7 @@ DHD void stage_b_update(const Mats& M, const State<NM, D>& U, const CellA<NM, D>
     enforce_positive_primitive<NM, D>(Ph);
 }
 
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Pe_lo,
                  const Prim<NM, D>& Pe_hi, bool end, int dir, double dt, double dx, State<NM, D>& Uh,
                  Prim<NM, D>& Ph)
@@ -139,9 +139,9 @@ DHD void stage_b(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
     Prim<NM, D> Pl, Pr;
     reconstruct_cell_faces<NM, D>(Pe_lo, A.Pe, Pe_hi, Pl, Pr);
     Flux<NM, D> FL, FR;
-    face_flux<NM, D>(M, Pl, dir, FL);
-    face_flux<NM, D>(M, Pr, dir, FR);
-    stage_b_update<NM, D>(M, U, A, Pl, Pr, FL, FR, dir, dt, dx, Uh, Ph);
+    face_flux<NM, D, IL>(M, Pl, dir, FL);
+    face_flux<NM, D, IL>(M, Pr, dir, FR);
+    stage_b_update<NM, D, IL>(M, U, A, Pl, Pr, FL, FR, dir, dt, dx, Uh, Ph);
 }
 
 // One face state of stage C: the conservative state of the reconstructed
@@ -157,7 +157,7 @@ DHD void face_state(const Mats& M, const Prim<NM, D>& Pf, State<NM, D>& S, Prim<
 // Stage C: the half-step face states of cell i (U_left_half[i],
 // U_right_half[i]) and their primitives (the cons_to_prim of PL_face /
 // PR_face and of hllc_flux_normal).
-template<int NM, int D>
+template<int NM, int D, bool IL = false>
 DHD void stage_c(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, const Prim<NM, D>& Ph,
                  const Prim<NM, D>& Ph_lo, const Prim<NM, D>& Ph_hi, bool end, State<NM, D>& LS,
                  State<NM, D>& RS, Prim<NM, D>& PLS, Prim<NM, D>& PRS)
@@ -171,8 +171,8 @@ DHD void stage_c(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
     }
     Prim<NM, D> Lh, Rh;
     reconstruct_cell_faces<NM, D>(Ph_lo, Ph, Ph_hi, Lh, Rh);
-    face_state<NM, D>(M, Lh, LS, PLS);
-    face_state<NM, D>(M, Rh, RS, PRS);
+    face_state<NM, D, IL>(M, Lh, LS, PLS);
+    face_state<NM, D, IL>(M, Rh, RS, PRS);
 }
 
 // Stage D output per face.
