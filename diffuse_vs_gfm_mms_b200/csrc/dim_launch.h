@@ -36,9 +36,10 @@ struct dimgpu_batch;
 #endif
 
 // Whether the batch kernels inline the FP64 stages' routines (the mixed
-// instances of a batch always call the out-of-line copies).
+// instances of a batch always call the out-of-line copies).  Measured on a
+// B200: c3 1.3 % more solves/s inlined.
 #ifndef DIMGPU_BATCH_INLINE
-#define DIMGPU_BATCH_INLINE false
+#define DIMGPU_BATCH_INLINE true
 #endif
 
 // Whether the staged D and E kernels inline their sound speeds and repairs

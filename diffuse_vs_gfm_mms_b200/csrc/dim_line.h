@@ -48,7 +48,7 @@ DHD State<NM, D> p2c(const Mats& M, const Prim<NM, D>& P)
 template<int NM, int D, bool IL>
 DHD State<NM, D> repair(const Mats& M, const State<NM, D>& U)
 {
-    if constexpr (IL) return repair_state_t<NM, D>(M, U);
+    if constexpr (IL) return repair_state_t<NM, D, false>(M, U);
     else return repair_state_v<NM, D>(M, U);
 }
 

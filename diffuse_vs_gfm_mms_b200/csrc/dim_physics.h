@@ -236,13 +236,20 @@ DHD MixVec<NM> mix_of(const double* alpha, const double* rho)
 }
 
 template<int NM>
-DHD double pressure_recover(const Mats& M, double rho_total, double e, MixVec<NM> x)
+DNI double pressure_from_internal_energy_v(const Mats& M, double rho_total, double e, MixVec<NM> x);
+
+// FULL = false is the inlined form: it carries only the certain-bracket
+// path, which every recovery of the benchmarked fields takes, and hands a
+// state without a certain bracket to the out-of-line full form (which
+// recomputes it from the same inputs: the same result, less inlined code).
+template<int NM, bool FULL = true>
+DHD double pressure_recover(const Mats& M, double rho_total_in, double e_in, MixVec<NM> x)
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
     DIMGPU_OPCOUNT(kOpRecover);
-    rho_total = clamp_min(rho_total);
-    e = finite_or(e);
+    double rho_total = clamp_min(rho_total_in);
+    double e = finite_or(e_in);
     const double target = finite_or(rho_total * e);
 
     double fallback_pressure = 0.0;
@@ -291,6 +298,9 @@ DHD double pressure_recover(const Mats& M, double rho_total, double e, MixVec<NM
         P_lo = P_lo - fabs(P_lo) * 1e-13 - 1e-300;
         P_fin = 1e290 * rA;
         fast = fin(P_hi) && fin(P_lo);
+    }
+    if constexpr (!FULL) {
+        if (!fast) return pressure_from_internal_energy_v<NM>(M, rho_total_in, e_in, x);
     }
     if (!fast) DIMGPU_OPCOUNT(kOpNotFast);
     // status: -1 certainly f < -thresh, +1 certainly f > thresh, 0 unknown
@@ -362,6 +372,9 @@ DHD double pressure_recover(const Mats& M, double rho_total, double e, MixVec<NM
     // change either decision (mid < 1e-10 is below P_lo clamped or not), so
     // the dependency chain of a step is add, multiply, compare, select.
     const bool fast_loop = fast && clamp_min(hi) < P_fin;
+    if constexpr (!FULL) {
+        if (!fast_loop) return pressure_from_internal_energy_v<NM>(M, rho_total_in, e_in, x);
+    }
     const bool no_clamp = fast_loop && P_lo > 1e-10;
     for (int n = 0; n < 80; ++n) {
         const double mid = 0.5 * (lo + hi);
@@ -547,7 +560,7 @@ DHD Prim<NM, D> cons_to_prim_t(const Mats& M, State<NM, D> U)
     const double kinetic = 0.5 * rho_total * velocity_squared;
     const double internal_energy = safe_div(finite_or(U.E, kinetic) - kinetic, rho_total);
     double p;
-    if constexpr (IL) p = pressure_recover<NM>(M, rho_total, internal_energy, mix_of<NM>(P.alpha, P.rho));
+    if constexpr (IL) p = pressure_recover<NM, false>(M, rho_total, internal_energy, mix_of<NM>(P.alpha, P.rho));
     else p = pressure_from_internal_energy<NM>(M, rho_total, internal_energy, P.alpha, P.rho);
     P.p = dmax(p, 1e-12);
     return P;
@@ -675,8 +688,14 @@ DHD void alpha_rhs_coefficients(const Mats& M, const Prim<NM, D>& P, const doubl
     }
 }
 
-// repair_state, primitives.hpp:325-457.
 template<int NM, int D>
+DNI State<NM, D> repair_state_v(const Mats& M, State<NM, D> U);
+
+// repair_state, primitives.hpp:325-457.  FULL = false is the inlined form:
+// it carries only the path where nothing is removed and E clears the energy
+// floor's bound, and hands every other state — after the input clamps,
+// which are idempotent — to the out-of-line full form.
+template<int NM, int D, bool FULL = true>
 DHD State<NM, D> repair_state_t(const Mats& M, State<NM, D> U)
 {
     DIMGPU_OPCOUNT(kOpRepair);
@@ -701,6 +720,29 @@ DHD State<NM, D> repair_state_t(const Mats& M, State<NM, D> U)
     for (int k = 0; k < NM; ++k) {
         remove[k] = alpha_full[k] <= inactive_alpha_floor && U.m[k] > mass_floor;
         removed_inactive_mass = removed_inactive_mass || remove[k];
+    }
+
+    if constexpr (!FULL) {
+        // the full form's steps below, on the path that removes nothing:
+        // the same total density, the same bound test, the same result
+        const double rho_total = total_density<NM, D>(U);
+        const double E = finite_or(U.E);
+        bool plain = !removed_inactive_mass && fin(rho_total) && rho_total > 0.0;
+        if (plain) {
+            double msq = 0.0;
+#pragma unroll
+            for (int d = 0; d < D; ++d) msq += U.mom[d] * U.mom[d];
+            double ub = 0.5 * msq / rho_total * (1.0 + 1e-12);
+#pragma unroll
+            for (int k = 0; k < NM; ++k) ub += dmax(alpha_full[k], 0.0) * M.einf_ub[k];
+            ub = ub * (1.0 + 1e-12) + 1e-290;
+            plain = fin(ub) && E >= ub;
+        }
+        if (!plain) return repair_state_v<NM, D>(M, U);
+#pragma unroll
+        for (int k = 0; k < NM - 1; ++k) U.a[k] = alpha_full[k];
+        U.E = E;
+        return U;
     }
 
     double velocity_before[D];

@@ -76,7 +76,9 @@ void load_prim(const double* in, Prim<NM, D>& P)
 }
 
 // One line through stages A..E (the kernel's tile schedule, untiled).
-template<int NM, int D>
+// IL = true: the inlined forms of the routines, as the staged kernels run
+// them (their common paths inline, the rest through the out-of-line forms).
+template<int NM, int D, bool IL = true>
 int solve_line_stages(const Mats& M, int n, const State<NM, D>* U, State<NM, D>* out, int dir, double dt,
                       double dx)
 {
@@ -89,23 +91,23 @@ int solve_line_stages(const Mats& M, int n, const State<NM, D>* U, State<NM, D>*
     std::vector<Prim<NM, D>> Ph(n), PLS(n), PRS(n);
     std::vector<FaceD<NM, D>> F(n);
     auto is_end = [&](int i) { return i == 0 || i == n - 1 || n < 3; };
-    for (int i = 0; i < n; ++i) stage_a<NM, D>(M, U[i], A[i]);
+    for (int i = 0; i < n; ++i) stage_a<NM, D, IL>(M, U[i], A[i]);
     for (int i = 0; i < n; ++i) {
         const Prim<NM, D>& lo = A[i > 0 ? i - 1 : i].Pe;
         const Prim<NM, D>& hi = A[i < n - 1 ? i + 1 : i].Pe;
-        stage_b<NM, D>(M, U[i], A[i], lo, hi, is_end(i), dir, dt, dx, Uh[i], Ph[i]);
+        stage_b<NM, D, IL>(M, U[i], A[i], lo, hi, is_end(i), dir, dt, dx, Uh[i], Ph[i]);
     }
     for (int i = 0; i < n; ++i) {
         const Prim<NM, D>& lo = Ph[i > 0 ? i - 1 : i];
         const Prim<NM, D>& hi = Ph[i < n - 1 ? i + 1 : i];
-        stage_c<NM, D>(M, U[i], A[i], Ph[i], lo, hi, is_end(i), LS[i], RS[i], PLS[i], PRS[i]);
+        stage_c<NM, D, IL>(M, U[i], A[i], Ph[i], lo, hi, is_end(i), LS[i], RS[i], PLS[i], PRS[i]);
     }
     for (int i = 0; i + 1 < n; ++i)
-        if (!stage_d<NM, D>(M, RS[i], PRS[i], LS[i + 1], PLS[i + 1], dir, F[i])) return DIMGPU_E_NONFINITE;
+        if (!stage_d<NM, D, IL>(M, RS[i], PRS[i], LS[i + 1], PLS[i + 1], dir, F[i])) return DIMGPU_E_NONFINITE;
     for (int i = 0; i < n; ++i) {
         const FaceD<NM, D>* lo = i > 0 ? &F[i - 1] : nullptr;
         const FaceD<NM, D>* hi = i < n - 1 ? &F[i] : nullptr;
-        stage_e<NM, D>(M, U[i], A[i], lo, hi, i == 0, i == n - 1, dt, dx, out[i]);
+        stage_e<NM, D, IL>(M, U[i], A[i], lo, hi, i == 0, i == n - 1, dt, dx, out[i]);
     }
     return 0;
 }
