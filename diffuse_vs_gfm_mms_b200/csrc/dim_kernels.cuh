@@ -836,6 +836,46 @@ __global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in
     g_put<NM, D>(b.F, b.cap, t, f);
 }
 
+// Stages C and D of the FP64 step fused, one thread per face i|i+1: the
+// right face state of cell i and the left one of cell i+1 are built (stage
+// C's reconstruction, build, repair, recovery, as face_state) and go
+// straight into HLLC, so the four face-state records never reach HBM.  Each
+// face state belongs to exactly one face, so nothing is computed twice.  The
+// two face states run through one inlined copy of the routines (a loop of
+// two, not unrolled); the first is parked in a small local array.
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+                                                 StagedBufs<NM, D> b, int* __restrict__ err)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)ls.nl * ls.n) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const int n = ls.n;
+    if (it.gi >= n - 1) return;  // face i|i+1 exists for i <= n-2
+    State<NM, D> S[2];
+    Prim<NM, D> P[2];
+#pragma unroll 1
+    for (int side = 0; side < 2; ++side) {
+        // side 0: cell i, its right face; side 1: cell i+1, its left face
+        const long long tc = t + side * it.s;
+        const int gi = it.gi + side;
+        if (gi == 0 || gi == n - 1 || n < 3) {
+            load_cell<NM, D>(in, g.ncell, it.cell + side * g.stride[DIR], S[side]);
+            g_get<NM, D>(b.P, b.cap, tc, P[side]);
+            continue;
+        }
+        Prim<NM, D> lo, c, hi, Lh, Rh;
+        g_get<NM, D>(b.Ph, b.cap, tc - it.s, lo);
+        g_get<NM, D>(b.Ph, b.cap, tc, c);
+        g_get<NM, D>(b.Ph, b.cap, tc + it.s, hi);
+        reconstruct_cell_faces<NM, D>(lo, c, hi, Lh, Rh);
+        face_state<NM, D, true>(M, side == 0 ? Rh : Lh, S[side], P[side]);
+    }
+    FaceD<NM, D> f;
+    if (!stage_d<NM, D, DIMGPU_STAGED_INLINE_DE>(M, S[0], P[0], S[1], P[1], DIR, f)) atomicOr(err, kErrNonFinite);
+    g_put<NM, D>(b.F, b.cap, t, f);
+}
+
 // dt = min(dt_max, slot) after a fused stage A; re-arms the slot to +inf.
 static __global__ void fused_cfl_finalize(unsigned long long* __restrict__ slot, double dt_max, double* __restrict__ dt,
                                    double* __restrict__ hist, int* __restrict__ err)
@@ -1252,10 +1292,16 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         count_launches(1);
         staged_bu<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
         count_launches(1);
-        staged_c<NM, D, DIR><<<blocks2, 256, 0, s>>>(in, g, M, ls, b);
-        count_launches(1);
-        staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
-        count_launches(1);
+        if (DIMGPU_STAGED_FUSE_CD) {
+            staged_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+            count_launches(1);
+        }
+        else {
+            staged_c<NM, D, DIR><<<blocks2, 256, 0, s>>>(in, g, M, ls, b);
+            count_launches(1);
+            staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
+            count_launches(1);
+        }
         staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
         count_launches(1);
         const cudaError_t e = cudaGetLastError();

@@ -42,6 +42,12 @@ struct dimgpu_batch;
 #define DIMGPU_BATCH_INLINE true
 #endif
 
+// Whether the staged schedule runs stages C and D as one kernel per face
+// (staged_cd) instead of staged_c + staged_d.
+#ifndef DIMGPU_STAGED_FUSE_CD
+#define DIMGPU_STAGED_FUSE_CD false
+#endif
+
 // Whether the staged D and E kernels inline their sound speeds and repairs
 // (two call sites each) instead of calling the out-of-line copies.
 // Measured on a B200: 1.5 % less time per step on c1 and c2 inlined.
