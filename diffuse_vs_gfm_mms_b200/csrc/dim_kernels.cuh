@@ -743,7 +743,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_e(const double
 // so the face states never reach HBM.  Scratch: P, ck, Pe, Ph and the face
 // records, at the staged positions.
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256) mixed_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                StagedBufs<NM, D> b, FusedCfl fc)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -28,6 +28,17 @@ struct dimgpu_batch;
 #define DIMGPU_FACE_MINB 4
 #endif
 
+// Whether the Euler sweep builds each cell's two face states through one
+// inlined copy of the routines (a loop of two) instead of two copies.
+#ifndef DIMGPU_EULER_FACE_LOOP
+#define DIMGPU_EULER_FACE_LOOP 0
+#endif
+
+// Resident blocks per SM mixed_a is compiled for (1: no register cap).
+#ifndef DIMGPU_MIXED_A_MINB
+#define DIMGPU_MIXED_A_MINB 1
+#endif
+
 // Whether the mixed-precision kernels (mixed_a, mixed_b, mixed_cd) inline
 // their recoveries, conversions, repairs and sound speeds.  Measured on a
 // B200: 2 % less time per step on c1, 3 % on c2 (512^3) inlined.

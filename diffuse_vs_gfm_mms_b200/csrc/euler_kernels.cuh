@@ -171,9 +171,18 @@ __global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __res
             e_get<D>(S0, NT, t + s, hi);
             EState<D> U, Uh;
             e_load<D>(in, g.ncell, cell, U);
+#if DIMGPU_EULER_FACE_LOOP
+            // both face states through one inlined copy (a loop of two, not
+            // unrolled): half the instruction footprint of two copies
+            EState<D> Uf[2];
+#pragma unroll 1
+            for (int side = 0; side < 2; ++side) Uf[side] = e_face_state<D>(M, lo, P, hi, side == 1);
+            ok &= e_hancock<D>(M, U, Uf[0], Uf[1], DIR, dt, dx, Uh);
+#else
             const EState<D> Ul = e_face_state<D>(M, lo, P, hi, false);
             const EState<D> Ur = e_face_state<D>(M, lo, P, hi, true);
             ok &= e_hancock<D>(M, U, Ul, Ur, DIR, dt, dx, Uh);
+#endif
             Ph = e_cons_to_prim<D>(M, Uh);
             e_enforce_prim<D>(Ph);
         }
@@ -189,6 +198,22 @@ __global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __res
     };
     const bool needC = needC_at(pos, gi);
     if (needC) {
+#if DIMGPU_EULER_FACE_LOOP
+        EPrim<D> lo, c, hi;
+        if (!end) {
+            e_get<D>(S1, NT, t - s, lo);
+            e_get<D>(S1, NT, t, c);
+            e_get<D>(S1, NT, t + s, hi);
+        }
+#pragma unroll 1
+        for (int side = 0; side < 2; ++side) {
+            EState<D> X;
+            if (end) e_load<D>(in, g.ncell, cell, X);
+            else X = e_face_state<D>(M, lo, c, hi, side == 1);
+            e_enforce<D>(M, X);
+            e_put<D>(side == 0 ? S2 : S0, NT, t, X);
+        }
+#else
         EState<D> LS, RS;
         if (end) {
             e_load<D>(in, g.ncell, cell, LS);
@@ -206,6 +231,7 @@ __global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __res
         e_enforce<D>(M, RS);
         e_put<D>(S2, NT, t, LS);
         e_put<D>(S0, NT, t, RS);
+#endif
     }
     __syncthreads();
 
