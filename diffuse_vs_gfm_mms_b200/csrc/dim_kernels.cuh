@@ -769,7 +769,7 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double
 // cut the mixed step's time on a B200 by 2.5 % (2D shock-bubble 1024x512)
 // and 1.2 % (3D bubble cloud 256^3).
 template<int NM, int D, int DIR, typename R = float>
-__global__ void __launch_bounds__(256, 3) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -816,7 +816,7 @@ __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const 
 }
 
 template<int NM, int D, int DIR, typename R = float>
-__global__ void __launch_bounds__(256, 3) mixed_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                    StagedBufs<NM, D> b, int* __restrict__ err)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
