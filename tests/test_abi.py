@@ -87,3 +87,27 @@ def test_slab_creator_refusals(lib):
     d = abi.make_desc(3, [8, 8, 11], [1 / 8] * 3, mats)
     assert create(d, 4)[0] == abi.E_INVALID_ARG
     assert create(d, 0)[0] == abi.E_INVALID_ARG
+
+
+def test_every_struct_layout_matches_header(tmp_path):
+    """ctypes field offsets and sizes == the C compiler's for every struct
+    the header passes by pointer (server configuration and counters,
+    initial-condition parameters, phase times)."""
+    import subprocess
+    pairs = [(abi.PhaseTimes, "dimgpu_phase_times"), (abi.ServerConfig, "dimgpu_server_config"),
+             (abi.ServerCounters, "dimgpu_server_counters"), (abi.ShockBubbleIC, "dimgpu_ic_shock_bubble"),
+             (abi.BubbleIC, "dimgpu_ic_bubble"), (abi.BubbleCloudIC, "dimgpu_ic_bubble_cloud")]
+    body, want = "", []
+    for cls, cname in pairs:
+        for f, _ in cls._fields_:
+            body += f'printf("%zu ", offsetof({cname}, {f}));'
+            want.append(getattr(cls, f).offset)
+        body += f'printf("%zu ", sizeof({cname}));'
+        want.append(C.sizeof(cls))
+    src = tmp_path / "layout2.c"
+    src.write_text('#include <stdio.h>\n#include <stddef.h>\n#include "dimgpu.h"\n'
+                   f'int main(void){{ {body} return 0; }}\n')
+    exe = tmp_path / "layout2"
+    subprocess.run(["gcc", f"-I{os.path.join(ROOT, 'include')}", str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True).stdout.split()]
+    assert got == want
