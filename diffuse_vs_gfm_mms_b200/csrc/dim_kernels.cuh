@@ -763,11 +763,10 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double
     if (fc.on) fused_cfl_reduce(best, fc);
 }
 
-// mixed_b and mixed_cd run 3 blocks of 256 threads per SM (at most 85
-// registers a thread, a few spilled to L1) rather than the 2 that ~100
-// registers allow: the FP64 chains are latency-bound, and the extra warps
-// cut the mixed step's time on a B200 by 2.5 % (2D shock-bubble 1024x512)
-// and 1.2 % (3D bubble cloud 256^3).
+// mixed_b and mixed_cd run DIMGPU_MIXED_BCD_MINB blocks of 256 threads per
+// SM (dim_launch.h) rather than the 2 that their ~100 registers allow: the
+// FP64 chains are latency-bound, and the extra warps hide more of them than
+// the few spills to L1 cost.
 template<int NM, int D, int DIR, typename R = float>
 __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)

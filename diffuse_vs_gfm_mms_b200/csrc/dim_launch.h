@@ -42,9 +42,10 @@ struct dimgpu_batch;
 #define DIMGPU_MIXED_A_MINB 3
 #endif
 
-// Resident blocks per SM of mixed_b and mixed_cd.
+// Resident blocks per SM of mixed_b and mixed_cd.  Measured on a B200: at 4
+// the mixed c2 step is 2.5 % faster than at 3, c1 unchanged.
 #ifndef DIMGPU_MIXED_BCD_MINB
-#define DIMGPU_MIXED_BCD_MINB 3
+#define DIMGPU_MIXED_BCD_MINB 4
 #endif
 
 // Whether the mixed-precision kernels (mixed_a, mixed_b, mixed_cd) inline
