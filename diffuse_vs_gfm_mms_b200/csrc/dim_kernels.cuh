@@ -503,6 +503,21 @@ __device__ __forceinline__ void g_get(const double* b, long long cap, long long 
     for (int k = 0; k < NM; ++k) f.af[k] = b[(v++) * cap + t];
 }
 
+// Stage A's enforced primitive of item t: the stored record, or (with
+// DIMGPU_STAGED_NO_PE) the primitive P re-enforced on load — the same bits
+// as stage A's enforce_positive_primitive, one record less written per cell.
+template<int NM, int D>
+__device__ __forceinline__ void get_pe(const StagedBufs<NM, D>& b, long long t, Prim<NM, D>& Pe)
+{
+    if (DIMGPU_STAGED_NO_PE) {
+        g_get<NM, D>(b.P, b.cap, t, Pe);
+        enforce_positive_primitive<NM, D>(Pe);
+    }
+    else {
+        g_get<NM, D>(b.Pe, b.cap, t, Pe);
+    }
+}
+
 // A face flux record (stage B's face fluxes, kept in the LS / RS slots until
 // stage C writes the face states there).
 template<int NM, int D>
@@ -589,7 +604,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double
         CellA<NM, D> A;
         stage_a<NM, D, true>(M, U, A);
         g_put<NM, D>(b.P, b.cap, t, A.P);
-        g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
+        if (!DIMGPU_STAGED_NO_PE) g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
         if (fc.on) best = cfl_candidate<NM, D, true>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
@@ -614,9 +629,9 @@ __global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_bf(__grid_consta
     const int n = ls.n;
     if (it.gi == 0 || it.gi == n - 1 || n < 3) return;  // end cells reconstruct nothing
     Prim<NM, D> lo, c, hi, Pl, Pr;
-    g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
-    g_get<NM, D>(b.Pe, b.cap, t, c);
-    g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+    get_pe<NM, D>(b, t - it.s, lo);
+    get_pe<NM, D>(b, t, c);
+    get_pe<NM, D>(b, t + it.s, hi);
     reconstruct_cell_faces<NM, D>(lo, c, hi, Pl, Pr);
     Flux<NM, D> F;
     face_flux<NM, D, true>(M, right ? Pr : Pl, DIR, F);
@@ -635,7 +650,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const doubl
     const int n = ls.n;
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
     CellA<NM, D> A;
-    g_get<NM, D>(b.Pe, b.cap, t, A.Pe);
+    get_pe<NM, D>(b, t, A.Pe);
     Prim<NM, D> Ph;
     if (end) {
         Ph = A.Pe;
@@ -646,8 +661,8 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const doubl
 #pragma unroll
         for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
         Prim<NM, D> lo, hi, Pl, Pr;
-        g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
-        g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+        get_pe<NM, D>(b, t - it.s, lo);
+        get_pe<NM, D>(b, t + it.s, hi);
         reconstruct_cell_faces<NM, D>(lo, A.Pe, hi, Pl, Pr);
         Flux<NM, D> FL, FR;
         g_get<NM, D>(b.LS, b.cap, t, FL);
@@ -755,7 +770,7 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double
         CellA<NM, D> A;
         stage_a_mixed<NM, D, DIMGPU_MIXED_INLINE>(M, U, A);
         g_put<NM, D>(b.P, b.cap, t, A.P);
-        g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
+        if (!DIMGPU_STAGED_NO_PE) g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
         if (fc.on) best = cfl_candidate<NM, D, DIMGPU_MIXED_INLINE>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
@@ -777,7 +792,7 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const doub
     const int n = ls.n;
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
     CellA<NM, D> A;
-    g_get<NM, D>(b.Pe, b.cap, t, A.Pe);
+    get_pe<NM, D>(b, t, A.Pe);
     Prim<NM, D> Ph;
     if (end) {
         Ph = A.Pe;
@@ -788,8 +803,8 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const doub
 #pragma unroll
         for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
         Prim<NM, D> lo, hi;
-        g_get<NM, D>(b.Pe, b.cap, t - it.s, lo);
-        g_get<NM, D>(b.Pe, b.cap, t + it.s, hi);
+        get_pe<NM, D>(b, t - it.s, lo);
+        get_pe<NM, D>(b, t + it.s, hi);
         stage_b_mixed<NM, D, R, DIMGPU_MIXED_INLINE>(M, U, A, lo, hi, false, DIR, *dtp, g.dx[DIR], Ph);
     }
     g_put<NM, D>(b.Ph, b.cap, t, Ph);

@@ -62,6 +62,12 @@ struct dimgpu_batch;
 #define DIMGPU_BATCH_INLINE true
 #endif
 
+// Whether stage A stores only the primitive P and the stage B kernels
+// re-enforce it on load, instead of storing the enforced copy as well.
+#ifndef DIMGPU_STAGED_NO_PE
+#define DIMGPU_STAGED_NO_PE false
+#endif
+
 // Whether the staged schedule runs stages C and D as one kernel per face
 // (staged_cd) instead of staged_c + staged_d.
 #ifndef DIMGPU_STAGED_FUSE_CD
