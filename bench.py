@@ -355,6 +355,49 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def run_slabs(args):
+    """One grid cut into `--slabs` slabs along its slowest axis
+    (dimgpu_slabs_*), every slab on its own GPU where the node has enough,
+    else several slabs per GPU; against one session on the whole grid.  Both
+    run the same steps; a slab step ends with a host synchronisation (the dt
+    minimum over the slabs), so both are timed with the wall clock around
+    synchronised steps."""
+    import time
+
+    import torch
+
+    from diffuse_vs_gfm_mms_b200.dim import Session, Slabs
+
+    d, U = make_workload(args.workload, args.scale)
+    cfl = WORKLOADS[args.workload][1]
+    ngpu = max(1, torch.cuda.device_count())
+    devices = [k % ngpu for k in range(args.slabs)]
+
+    def timed(obj):
+        obj.steps(args.warmup, cfl, 1e300)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            obj.step(cfl, 1e300)
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / args.steps
+
+    with Session(d, U) as s:
+        one = timed(s)
+    with Slabs(d, devices, U) as L:
+        sl = timed(L)
+    line = {
+        "metric": METRIC, "value": d.ncell / sl, "unit": UNIT, "n_gpus": len(set(devices)), "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": sl * 1e3, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOADS[args.workload][0], "cells": d.ncell, "slabs": args.slabs,
+                   "devices": devices, "parallelism": f"slabs x{args.slabs}"},
+        "one_session": {"value": d.ncell / one, "ms_per_step": one * 1e3},
+        "timing": "wall clock around host-synchronised steps (both arms)",
+    }
+    print(json.dumps(line), flush=True)
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -769,6 +812,7 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--schedule", default="staged", choices=["staged", "fused"],
                     help="sweep schedule of the FP64 step (fused: one tile kernel per sweep)")
+    ap.add_argument("--slabs", type=int, default=0, help="cut the grid into this many slabs (dimgpu_slabs_*)")
     ap.add_argument("--c3-steps", type=int, default=500)
     ap.add_argument("--c3-instances", type=int, default=256)
     ap.add_argument("--c3-sequential", type=int, default=16, help="instances in the sequential sample")
@@ -781,6 +825,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.slabs > 0:
+        run_slabs(args)
     elif args.workload == "c3":
         run_batch(args)
     elif args.workload == "c4":
