@@ -64,6 +64,8 @@ struct dimgpu_batch;
 
 // Whether stage A stores only the primitive P and the stage B kernels
 // re-enforce it on load, instead of storing the enforced copy as well.
+// Measured on a B200: FP64 c1 unchanged, c2 3 % slower (the enforce's
+// instructions cost more than the record's traffic saves), so off.
 #ifndef DIMGPU_STAGED_NO_PE
 #define DIMGPU_STAGED_NO_PE false
 #endif
