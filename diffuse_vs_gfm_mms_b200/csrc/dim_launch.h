@@ -28,6 +28,12 @@ struct dimgpu_batch;
 #define DIMGPU_FACE_MINB 4
 #endif
 
+// Resident 256-thread blocks per SM the Euler sweep is compiled for (its
+// register budget): 4, 64 registers.
+#ifndef DIMGPU_EULER_MINB
+#define DIMGPU_EULER_MINB 4
+#endif
+
 // Whether the Euler sweep builds each cell's two face states through one
 // inlined copy of the routines (a loop of two) instead of two copies.
 // Measured on a B200: 3 % (e2) and 5 % (e3) slower, so off.

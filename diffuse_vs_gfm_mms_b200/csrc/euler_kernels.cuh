@@ -101,7 +101,7 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // sweep is latency-bound on dependent FP64 chains; the extra warps hide more
 // of that latency than the few spilled registers (L1-resident) cost.
 template<int D, int DIR>
-__global__ void __launch_bounds__(256, 4) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
+__global__ void __launch_bounds__(256, DIMGPU_EULER_MINB) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                              __grid_constant__ const Grid g, __grid_constant__ const Mats M, int T, int W, int ntile, int ngx,
                                                              const double* __restrict__ dtp, int* __restrict__ err,
                                                              int ends_copy)
