@@ -8,6 +8,7 @@
 
 #include <cuda.h>
 #include <cstring>
+#include <utility>
 #include <cuda_runtime.h>
 
 #include "dim_launch.h"
@@ -564,6 +565,20 @@ struct StagedItem {
 };
 
 
+// Programmatic dependent launch of the staged kernels (DIMGPU_PDL): a
+// stage kernel launched with programmatic stream serialization may be
+// scheduled while its predecessor drains.  Every such kernel waits at its
+// very top (griddepcontrol.wait: the predecessor has completed and its
+// writes are visible) before anything else, so each kernel still completes
+// after its predecessor, and then lets its own successor be scheduled early.
+__device__ __forceinline__ void pdl_enter()
+{
+    if (DIMGPU_PDL) {
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    }
+}
+
 // Optional CFL reduction fused into stage A of the first sweep of a step:
 // stage A recovers every cell's primitive from the very state the CFL
 // minimum is taken over, so the candidate costs one sound speed, not a
@@ -595,6 +610,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b, FusedCfl fc)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double best = HUGE_VAL;
     if (t < (long long)ls.nl * ls.n) {
@@ -620,6 +636,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_bf(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                  StagedBufs<NM, D> b)
 {
+    pdl_enter();
     const long long N = (long long)ls.nl * ls.n;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * N) return;
@@ -644,6 +661,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                  StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -679,6 +697,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_c(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b)
 {
+    pdl_enter();
     const long long N = (long long)ls.nl * ls.n;
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= 2 * N) return;
@@ -709,6 +728,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_d(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 int* __restrict__ err)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -729,6 +749,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_e(const double
                                                 __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 const double* __restrict__ dtp)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -861,6 +882,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                  StagedBufs<NM, D> b, int* __restrict__ err)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -1267,6 +1289,28 @@ cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const
     return cudaErrorInvalidValue;
 }
 
+// Launch of a stage kernel; with DIMGPU_PDL it may be scheduled while the
+// previous kernel of the stream drains (pdl_enter orders the work).
+template<typename... KArgs, typename... Args>
+cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s, Args&&... args)
+{
+    if (!DIMGPU_PDL) {
+        kern<<<blocks, 256, 0, s>>>(std::forward<Args>(args)...);
+        return cudaSuccess;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(blocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
 // Staged schedule: chunks of whole lines, at most `cap` cells each; scratch
 // holds kStagedVars(NM, D) * cap doubles.
 template<int NM, int D, int DIR>
@@ -1302,21 +1346,21 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         count_launches(1);
         if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
         const unsigned blocks2 = (unsigned)((2 * items + 255) / 256);
-        staged_bf<NM, D, DIR><<<blocks2, 256, 0, s>>>(g, M, ls, b);
+        launch_stage(staged_bf<NM, D, DIR>, blocks2, s, g, M, ls, b);
         count_launches(1);
-        staged_bu<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
+        launch_stage(staged_bu<NM, D, DIR>, blocks, s, in, g, M, ls, b, dt);
         count_launches(1);
         if (DIMGPU_STAGED_FUSE_CD) {
-            staged_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+            launch_stage(staged_cd<NM, D, DIR>, blocks, s, in, g, M, ls, b, err);
             count_launches(1);
         }
         else {
-            staged_c<NM, D, DIR><<<blocks2, 256, 0, s>>>(in, g, M, ls, b);
+            launch_stage(staged_c<NM, D, DIR>, blocks2, s, in, g, M, ls, b);
             count_launches(1);
-            staged_d<NM, D, DIR><<<blocks, 256, 0, s>>>(g, M, ls, b, err);
+            launch_stage(staged_d<NM, D, DIR>, blocks, s, g, M, ls, b, err);
             count_launches(1);
         }
-        staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
+        launch_stage(staged_e<NM, D, DIR>, blocks, s, in, out, g, M, ls, b, dt);
         count_launches(1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;

@@ -76,6 +76,12 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_NO_PE false
 #endif
 
+// Whether the staged kernels after stage A are launched with programmatic
+// stream serialization (scheduled while their predecessor drains).
+#ifndef DIMGPU_PDL
+#define DIMGPU_PDL false
+#endif
+
 // Whether the staged schedule runs stages C and D as one kernel per face
 // (staged_cd) instead of staged_c + staged_d.
 #ifndef DIMGPU_STAGED_FUSE_CD
