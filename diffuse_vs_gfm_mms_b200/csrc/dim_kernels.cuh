@@ -782,6 +782,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                StagedBufs<NM, D> b, FusedCfl fc)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     double best = HUGE_VAL;
     if (t < (long long)ls.nl * ls.n) {
@@ -807,6 +808,7 @@ template<int NM, int D, int DIR, typename R = float>
 __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                   StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -854,6 +856,7 @@ template<int NM, int D, int DIR, typename R = float>
 __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_cd(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                    StagedBufs<NM, D> b, int* __restrict__ err)
 {
+    pdl_enter();
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= (long long)ls.nl * ls.n) return;
     const StagedItem<DIR> it(g, ls, t);
@@ -916,6 +919,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_cd(const doubl
 static __global__ void fused_cfl_finalize(unsigned long long* __restrict__ slot, double dt_max, double* __restrict__ dt,
                                    double* __restrict__ hist, int* __restrict__ err)
 {
+    pdl_enter();
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     const double m = __longlong_as_double((long long)*slot);
     const double d = dmin(dt_max, m);
@@ -1078,6 +1082,7 @@ template<int NM, int D>
 __global__ void __launch_bounds__(256) bc_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, long long plane0, long long plane1,
                                                  long long plane2)
 {
+    pdl_enter();
     const long long count[3] = {plane0, plane1, plane2};
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int a = 0;
@@ -1292,15 +1297,16 @@ cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const
 // Launch of a stage kernel; with DIMGPU_PDL it may be scheduled while the
 // previous kernel of the stream drains (pdl_enter orders the work).
 template<typename... KArgs, typename... Args>
-cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s, Args&&... args)
+cudaError_t launch_stage_dims(void (*kern)(KArgs...), unsigned blocks, unsigned threads, cudaStream_t s,
+                              Args&&... args)
 {
     if (!DIMGPU_PDL) {
-        kern<<<blocks, 256, 0, s>>>(std::forward<Args>(args)...);
+        kern<<<blocks, threads, 0, s>>>(std::forward<Args>(args)...);
         return cudaSuccess;
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(256);
+    cfg.blockDim = dim3(threads);
     cfg.dynamicSmemBytes = 0;
     cfg.stream = s;
     cudaLaunchAttribute attr[1];
@@ -1309,6 +1315,12 @@ cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
+}
+
+template<typename... KArgs, typename... Args>
+cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s, Args&&... args)
+{
+    return launch_stage_dims(kern, blocks, 256u, s, std::forward<Args>(args)...);
 }
 
 // Staged schedule: chunks of whole lines, at most `cap` cells each; scratch
@@ -1342,9 +1354,12 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         const unsigned blocks = (unsigned)((items + 255) / 256);
         FusedCfl fc{0, 0, 0.0, nullptr};
         if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
-        staged_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
+        launch_stage(staged_a<NM, D, DIR>, blocks, s, in, g, M, ls, b, fc);
         count_launches(1);
-        if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
+        if (fs.on) {
+            launch_stage_dims(fused_cfl_finalize, 1u, 1u, s, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err);
+            count_launches(1);
+        }
         const unsigned blocks2 = (unsigned)((2 * items + 255) / 256);
         launch_stage(staged_bf<NM, D, DIR>, blocks2, s, g, M, ls, b);
         count_launches(1);
@@ -1411,19 +1426,22 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
         const unsigned blocks = (unsigned)((items + 255) / 256);
         FusedCfl fc{0, 0, 0.0, nullptr};
         if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
-        mixed_a<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, fc);
+        launch_stage(mixed_a<NM, D, DIR>, blocks, s, in, g, M, ls, b, fc);
         count_launches(1);
-        if (fs.on) { fused_cfl_finalize<<<1, 1, 0, s>>>(fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err); count_launches(1); }
+        if (fs.on) {
+            launch_stage_dims(fused_cfl_finalize, 1u, 1u, s, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err);
+            count_launches(1);
+        }
         if (twin) {
-            mixed_b<NM, D, DIR, double><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
-            mixed_cd<NM, D, DIR, double><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+            launch_stage(mixed_b<NM, D, DIR, double>, blocks, s, in, g, M, ls, b, dt);
+            launch_stage(mixed_cd<NM, D, DIR, double>, blocks, s, in, g, M, ls, b, err);
         }
         else {
-            mixed_b<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, dt);
-            mixed_cd<NM, D, DIR><<<blocks, 256, 0, s>>>(in, g, M, ls, b, err);
+            launch_stage(mixed_b<NM, D, DIR>, blocks, s, in, g, M, ls, b, dt);
+            launch_stage(mixed_cd<NM, D, DIR>, blocks, s, in, g, M, ls, b, err);
         }
         count_launches(2);
-        staged_e<NM, D, DIR><<<blocks, 256, 0, s>>>(in, out, g, M, ls, b, dt);
+        launch_stage(staged_e<NM, D, DIR>, blocks, s, in, out, g, M, ls, b, dt);
         count_launches(1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -1493,7 +1511,7 @@ cudaError_t launch_bc(const Grid& g, const Mats& M, double* state, cudaStream_t 
         total += 2 * c;
     }
     if (total == 0) return cudaSuccess;
-    bc_kernel<NM, D><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(state, g, M, plane[0], plane[1], plane[2]);
+    launch_stage(bc_kernel<NM, D>, (unsigned)((total + 255) / 256), s, state, g, M, plane[0], plane[1], plane[2]);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -29,9 +29,10 @@ struct dimgpu_batch;
 #endif
 
 // Resident 256-thread blocks per SM the Euler sweep is compiled for (its
-// register budget): 4, 64 registers.
+// register budget).  Measured on a B200: 5 (51 registers) 1 % faster on e2
+// than 4, 3 slower.
 #ifndef DIMGPU_EULER_MINB
-#define DIMGPU_EULER_MINB 4
+#define DIMGPU_EULER_MINB 5
 #endif
 
 // Whether the Euler sweep builds each cell's two face states through one
@@ -76,10 +77,13 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_NO_PE false
 #endif
 
-// Whether the staged kernels after stage A are launched with programmatic
-// stream serialization (scheduled while their predecessor drains).
+// Whether the kernels of a session's step (the staged and mixed stages, the
+// fused-CFL finalize, the boundary fill) are launched with programmatic
+// stream serialization: each may be scheduled while its predecessor drains
+// and waits at its top for the predecessor's completion.  Measured on a
+// B200: c1 3.7 % less time per step.
 #ifndef DIMGPU_PDL
-#define DIMGPU_PDL false
+#define DIMGPU_PDL true
 #endif
 
 // Whether the staged schedule runs stages C and D as one kernel per face
