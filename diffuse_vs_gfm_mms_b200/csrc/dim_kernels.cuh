@@ -607,7 +607,7 @@ __device__ __forceinline__ void fused_cfl_reduce(double best, const FusedCfl& c)
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_A_MINB) staged_a(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                 StagedBufs<NM, D> b, FusedCfl fc)
 {
     pdl_enter();
@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_bf(__grid_consta
 // staged_bu: one thread per cell, the half-step update from the two face
 // fluxes (the face primitives are reconstructed again: the same values).
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_bu(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+__global__ void __launch_bounds__(256, DIMGPU_BU_MINB) staged_bu(const double* __restrict__ in, __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
                                                  StagedBufs<NM, D> b, const double* __restrict__ dtp)
 {
     pdl_enter();
@@ -725,7 +725,7 @@ __global__ void __launch_bounds__(256, DIMGPU_FACE_MINB) staged_c(const double* 
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_d(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
+__global__ void __launch_bounds__(256, DIMGPU_D_MINB) staged_d(__grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 int* __restrict__ err)
 {
     pdl_enter();
@@ -745,7 +745,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_d(__grid_const
 }
 
 template<int NM, int D, int DIR>
-__global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_e(const double* __restrict__ in, double* __restrict__ out, __grid_constant__ const Grid g,
+__global__ void __launch_bounds__(256, DIMGPU_E_MINB) staged_e(const double* __restrict__ in, double* __restrict__ out, __grid_constant__ const Grid g,
                                                 __grid_constant__ const Mats M, LineSet ls, StagedBufs<NM, D> b,
                                                 const double* __restrict__ dtp)
 {

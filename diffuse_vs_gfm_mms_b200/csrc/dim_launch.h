@@ -21,6 +21,20 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_MINB 3
 #endif
 
+// Per-kernel resident blocks per SM of stages A, B's cell update, D and E.
+#ifndef DIMGPU_A_MINB
+#define DIMGPU_A_MINB DIMGPU_STAGED_MINB
+#endif
+#ifndef DIMGPU_BU_MINB
+#define DIMGPU_BU_MINB DIMGPU_STAGED_MINB
+#endif
+#ifndef DIMGPU_D_MINB
+#define DIMGPU_D_MINB DIMGPU_STAGED_MINB
+#endif
+#ifndef DIMGPU_E_MINB
+#define DIMGPU_E_MINB DIMGPU_STAGED_MINB
+#endif
+
 // Resident blocks per SM of the per-face-state kernels (staged_bf, staged_c),
 // whose threads carry one face state each: 64 registers.  Measured on a
 // B200: 3.5 % less time per step on c2 (512^3) than at 3 blocks, 0.3 % on c1.
