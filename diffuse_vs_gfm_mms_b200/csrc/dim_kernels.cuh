@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include "dim_launch.h"
+#include "pdl.cuh"
 #include "dim_line.h"
 #include "dim_mixed.h"
 #include "dimgpu.h"
@@ -564,20 +565,6 @@ struct StagedItem {
     }
 };
 
-
-// Programmatic dependent launch of the staged kernels (DIMGPU_PDL): a
-// stage kernel launched with programmatic stream serialization may be
-// scheduled while its predecessor drains.  Every such kernel waits at its
-// very top (griddepcontrol.wait: the predecessor has completed and its
-// writes are visible) before anything else, so each kernel still completes
-// after its predecessor, and then lets its own successor be scheduled early.
-__device__ __forceinline__ void pdl_enter()
-{
-    if (DIMGPU_PDL) {
-        asm volatile("griddepcontrol.wait;" ::: "memory");
-        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-    }
-}
 
 // Optional CFL reduction fused into stage A of the first sweep of a step:
 // stage A recovers every cell's primitive from the very state the CFL
@@ -1292,35 +1279,6 @@ cudaError_t launch_sweep(const Grid& g, const Mats& M, int dir, Tile tile, const
         if (dir == 2) return launch_sweep_dir<NM, D, 2>(g, M, tile, in, out, dt, err, s);
     }
     return cudaErrorInvalidValue;
-}
-
-// Launch of a stage kernel; with DIMGPU_PDL it may be scheduled while the
-// previous kernel of the stream drains (pdl_enter orders the work).
-template<typename... KArgs, typename... Args>
-cudaError_t launch_stage_dims(void (*kern)(KArgs...), unsigned blocks, unsigned threads, cudaStream_t s,
-                              Args&&... args)
-{
-    if (!DIMGPU_PDL) {
-        kern<<<blocks, threads, 0, s>>>(std::forward<Args>(args)...);
-        return cudaSuccess;
-    }
-    cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(blocks);
-    cfg.blockDim = dim3(threads);
-    cfg.dynamicSmemBytes = 0;
-    cfg.stream = s;
-    cudaLaunchAttribute attr[1];
-    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    attr[0].val.programmaticStreamSerializationAllowed = 1;
-    cfg.attrs = attr;
-    cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...);
-}
-
-template<typename... KArgs, typename... Args>
-cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s, Args&&... args)
-{
-    return launch_stage_dims(kern, blocks, 256u, s, std::forward<Args>(args)...);
 }
 
 // Staged schedule: chunks of whole lines, at most `cap` cells each; scratch

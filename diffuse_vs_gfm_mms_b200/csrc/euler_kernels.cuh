@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "dim_launch.h"
+#include "pdl.cuh"
 #include "euler_physics.h"
 #include "dimgpu.h"
 
@@ -106,6 +107,7 @@ __global__ void __launch_bounds__(256, DIMGPU_EULER_MINB) euler_sweep_kernel(con
                                                              const double* __restrict__ dtp, int* __restrict__ err,
                                                              int ends_copy)
 {
+    pdl_enter();
     extern __shared__ double sm[];
     const int NT = T * W;
     double* S0 = sm;
@@ -276,6 +278,7 @@ __global__ void __launch_bounds__(256) euler_cfl_kernel(const double* __restrict
                                                         int unsplit, double* __restrict__ blockmin,
                                                         int* __restrict__ err)
 {
+    pdl_enter();
     __shared__ double red[32];
     double best = HUGE_VAL;
     bool ok = true;
@@ -399,6 +402,7 @@ template<int D>
 __global__ void __launch_bounds__(256) euler_bc_kernel(double* st, __grid_constant__ const Grid g, __grid_constant__ const Mats M, long long plane0,
                                                        long long plane1, long long plane2)
 {
+    pdl_enter();
     const long long count[3] = {plane0, plane1, plane2};
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int a = 0;
@@ -488,7 +492,8 @@ cudaError_t launch_euler_sweep_dir(const Grid& g, const Mats& M, Tile tile, cons
     auto kern = euler_sweep_kernel<D, DIR>;
     const cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ea != cudaSuccess) return ea;
-    kern<<<(unsigned)nblocks, T * W, smem, s>>>(in, out, g, M, T, W, ntile, ngx, dt, err, ends_copy);
+    launch_stage_smem(kern, (unsigned)nblocks, (unsigned)(T * W), smem, s, in, out, g, M, T, W, ntile, ngx, dt, err,
+                      ends_copy);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -516,7 +521,7 @@ cudaError_t launch_euler_cfl(const Grid& g, const Mats& M, const double* state, 
     if (nb > max_blocks) nb = max_blocks;
     if (nb < 1) nb = 1;
     *nblocks = (int)nb;
-    euler_cfl_kernel<D><<<(unsigned)nb, 256, 0, s>>>(state, g, M, cfl, unsplit ? 1 : 0, blockmin, err);
+    launch_stage(euler_cfl_kernel<D>, (unsigned)nb, s, state, g, M, cfl, unsplit ? 1 : 0, blockmin, err);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -546,7 +551,7 @@ cudaError_t launch_euler_bc(const Grid& g, const Mats& M, double* state, cudaStr
         total += 2 * c;
     }
     if (total == 0) return cudaSuccess;
-    euler_bc_kernel<D><<<(unsigned)((total + 255) / 256), 256, 0, s>>>(state, g, M, plane[0], plane[1], plane[2]);
+    launch_stage(euler_bc_kernel<D>, (unsigned)((total + 255) / 256), s, state, g, M, plane[0], plane[1], plane[2]);
     count_launches(1);
     return cudaGetLastError();
 }
