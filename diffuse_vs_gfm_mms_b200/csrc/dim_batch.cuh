@@ -45,6 +45,7 @@ template<int NM, int D>
 __global__ void __launch_bounds__(256) batch_cfl(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                  int ninst, double* __restrict__ blockmin)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     __shared__ double red[8];
     const long long total = prefix[ninst];
     for (long long wb = blockIdx.x; wb < total; wb += gridDim.x) {
@@ -80,6 +81,7 @@ __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__ tab, c
                                                       int ninst, const double* __restrict__ blockmin,
                                                       int* __restrict__ err)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     __shared__ double red[8];
     for (int i = blockIdx.x; i < ninst; i += gridDim.x) {
         double v = HUGE_VAL;
@@ -133,6 +135,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_a(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1) continue;
     State<NM, D> U;
@@ -151,6 +154,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_b(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1) continue;
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
@@ -184,6 +188,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_c(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1 || I.mixed) continue;  // mixed instances build their face states in batch_d
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
@@ -215,6 +220,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_d(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b, int* __restrict__ err)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     BATCH_LOOP_BEGIN
     if (!I.run || n == 1 || it.gi >= n - 1) continue;
     State<NM, D> UL, UR;
@@ -246,6 +252,7 @@ template<int NM, int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_e(const BInst* __restrict__ tab, const long long* __restrict__ prefix,
                                                int ninst, int rel, StagedBufs<NM, D> b)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     BATCH_LOOP_BEGIN
     if (!I.run) continue;
     double* out = I.st[I.cur ^ rel ^ 1];
@@ -276,6 +283,7 @@ template<int NM, int D>
 __global__ void __launch_bounds__(256) batch_bc(const BInst* __restrict__ tab, const long long* __restrict__ bprefix,
                                                 int ninst, int rel)
 {
+    pdl_enter_if<DIMGPU_BATCH_PDL>();
     const long long total = bprefix[ninst];
     for (long long wb = blockIdx.x; wb < total; wb += gridDim.x) {
         const int inst = batch_find(bprefix, ninst, wb);
@@ -330,17 +338,19 @@ cudaError_t batch_step(const BatchLaunch& L, cudaStream_t s)
     b.PLS = p; p += kPrimVars(NM, D) * L.cap;
     b.PRS = p; p += kPrimVars(NM, D) * L.cap;
     b.F = p;
-    batch_cfl<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, L.blockmin);
-    batch_finalize<D><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, L.blockmin, L.err);
+    launch_chained<DIMGPU_BATCH_PDL>(batch_cfl<NM, D>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, L.blockmin);
+    launch_chained<DIMGPU_BATCH_PDL>(batch_finalize<D>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, L.blockmin,
+                                     L.err);
     // sweep k reads st[cur ^ (k & 1)]; the boundary fill after it works on the
     // buffer it wrote, st[cur ^ (k & 1) ^ 1]
 #define BATCH_DIR(DIR)                                                                                   \
-    batch_a<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
-    batch_b<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
-    batch_c<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
-    batch_d<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b, L.err);        \
-    batch_e<NM, D, DIR><<<L.grid, 256, 0, s>>>(L.tab, L.cell_prefix, L.ninst, DIR & 1, b);               \
-    batch_bc<NM, D><<<L.grid, 256, 0, s>>>(L.tab, L.bc_prefix, L.ninst, (DIR & 1) ^ 1);
+    launch_chained<DIMGPU_BATCH_PDL>(batch_a<NM, D, DIR>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, DIR & 1, b); \
+    launch_chained<DIMGPU_BATCH_PDL>(batch_b<NM, D, DIR>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, DIR & 1, b); \
+    launch_chained<DIMGPU_BATCH_PDL>(batch_c<NM, D, DIR>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, DIR & 1, b); \
+    launch_chained<DIMGPU_BATCH_PDL>(batch_d<NM, D, DIR>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, DIR & 1, b,   \
+                                     L.err);                                                            \
+    launch_chained<DIMGPU_BATCH_PDL>(batch_e<NM, D, DIR>, L.grid, 256u, 0, s, L.tab, L.cell_prefix, L.ninst, DIR & 1, b); \
+    launch_chained<DIMGPU_BATCH_PDL>(batch_bc<NM, D>, L.grid, 256u, 0, s, L.tab, L.bc_prefix, L.ninst, (DIR & 1) ^ 1);
     BATCH_DIR(0)
     if constexpr (D >= 2) { BATCH_DIR(1) }
     if constexpr (D >= 3) { BATCH_DIR(2) }

@@ -102,6 +102,12 @@ struct dimgpu_batch;
 #define DIMGPU_PDL true
 #endif
 
+// Whether the batch step's kernels (captured into the batch's CUDA graph)
+// form a programmatic launch chain as well.
+#ifndef DIMGPU_BATCH_PDL
+#define DIMGPU_BATCH_PDL false
+#endif
+
 // Whether the staged schedule runs stages C and D as one kernel per face
 // (staged_cd) instead of staged_c + staged_d.
 #ifndef DIMGPU_STAGED_FUSE_CD

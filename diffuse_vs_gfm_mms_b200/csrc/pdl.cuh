@@ -17,20 +17,23 @@
 
 namespace dimgpu {
 
-__device__ __forceinline__ void pdl_enter()
+template<bool On>
+__device__ __forceinline__ void pdl_enter_if()
 {
-    if (DIMGPU_PDL) {
+    if (On) {
         asm volatile("griddepcontrol.wait;" ::: "memory");
         asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
     }
 }
 
-// Launch with programmatic stream serialization (plainly without DIMGPU_PDL).
-template<typename... KArgs, typename... Args>
-cudaError_t launch_stage_smem(void (*kern)(KArgs...), unsigned blocks, unsigned threads, size_t smem, cudaStream_t s,
-                              Args&&... args)
+__device__ __forceinline__ void pdl_enter() { pdl_enter_if<DIMGPU_PDL>(); }
+
+// Launch with programmatic stream serialization when On (plainly otherwise).
+template<bool On, typename... KArgs, typename... Args>
+cudaError_t launch_chained(void (*kern)(KArgs...), unsigned blocks, unsigned threads, size_t smem, cudaStream_t s,
+                           Args&&... args)
 {
-    if (!DIMGPU_PDL) {
+    if (!On) {
         kern<<<blocks, threads, smem, s>>>(std::forward<Args>(args)...);
         return cudaSuccess;
     }
@@ -48,16 +51,23 @@ cudaError_t launch_stage_smem(void (*kern)(KArgs...), unsigned blocks, unsigned 
 }
 
 template<typename... KArgs, typename... Args>
+cudaError_t launch_stage_smem(void (*kern)(KArgs...), unsigned blocks, unsigned threads, size_t smem, cudaStream_t s,
+                              Args&&... args)
+{
+    return launch_chained<DIMGPU_PDL>(kern, blocks, threads, smem, s, std::forward<Args>(args)...);
+}
+
+template<typename... KArgs, typename... Args>
 cudaError_t launch_stage_dims(void (*kern)(KArgs...), unsigned blocks, unsigned threads, cudaStream_t s,
                               Args&&... args)
 {
-    return launch_stage_smem(kern, blocks, threads, 0, s, std::forward<Args>(args)...);
+    return launch_chained<DIMGPU_PDL>(kern, blocks, threads, 0, s, std::forward<Args>(args)...);
 }
 
 template<typename... KArgs, typename... Args>
 cudaError_t launch_stage(void (*kern)(KArgs...), unsigned blocks, cudaStream_t s, Args&&... args)
 {
-    return launch_stage_smem(kern, blocks, 256u, 0, s, std::forward<Args>(args)...);
+    return launch_chained<DIMGPU_PDL>(kern, blocks, 256u, 0, s, std::forward<Args>(args)...);
 }
 
 }  // namespace dimgpu
