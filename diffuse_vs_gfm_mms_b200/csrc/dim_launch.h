@@ -103,7 +103,8 @@ struct dimgpu_batch;
 #endif
 
 // Whether the batch step's kernels (captured into the batch's CUDA graph)
-// form a programmatic launch chain as well.
+// form a programmatic launch chain as well.  Measured on a B200: no change
+// on c3 (44.4 ms batched steps), so off.
 #ifndef DIMGPU_BATCH_PDL
 #define DIMGPU_BATCH_PDL false
 #endif
