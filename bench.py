@@ -756,7 +756,8 @@ def run_serving(args):
     with ClockSampler(local) as clk:
         for rate in args.c4_rates:
             reqs = serve.make_requests(args.c4_requests, rate, seed=7 + rank)
-            with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8) as srv:
+            with serve.Server(hbm_budget_bytes=150e9, max_slots=args.c4_slots, quantum=8,
+                              solo_min_cells=args.c4_solo_min_cells, solo_slots=args.c4_solo_slots) as srv:
                 st = srv.serve(reqs)
             p50, p99 = st.latency_percentiles()
             svc = [service(r) for r in reqs]
@@ -791,6 +792,7 @@ def run_serving(args):
             "data": "synthetic",
             "config": {"workload": WORKLOADS["c4"][0],
                        "requests_per_rate": args.c4_requests, "rates": args.c4_rates,
+                       "solo_min_cells": args.c4_solo_min_cells, "solo_slots": args.c4_solo_slots,
                        "sample": f"{args.c4_requests} requests per rate of the 10,000-request stream"},
             "rates": rows,
             "speedup_vs_sequential_plain": best["served"]["solves_per_s"] / best["sequential_plain"]["solves_per_s"],
@@ -819,6 +821,8 @@ def main():
     ap.add_argument("--c4-requests", type=int, default=32)
     ap.add_argument("--c4-rates", type=float, nargs="+", default=[0.5, 1.0, 2.0, 4.0])
     ap.add_argument("--c4-slots", type=int, default=128)
+    ap.add_argument("--c4-solo-min-cells", type=int, default=1 << 18, help="solves this large run on solo lanes")
+    ap.add_argument("--c4-solo-slots", type=int, default=4)
     ap.add_argument("--c4-seq-every", type=int, default=8, help="sequential sample: every k-th request")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
