@@ -572,11 +572,20 @@ struct StagedItem {
 // second recovery.  Block minima go to one slot by atomicMin on the bit
 // pattern (every candidate is a non-negative double or +inf, which order
 // like their bits).
+// The last block to add its minimum (a ticket counter beside the slot)
+// also finishes the reduction — dt = min(dt_max, slot), the dt log, the
+// non-positive-dt flag — and re-arms slot and counter for the next step, so
+// no separate finalize kernel runs (the threadFenceReduction pattern: no
+// block waits for another).
 struct FusedCfl {
     int on;
     int unsplit;
     double cfl;
-    unsigned long long* slot;
+    unsigned long long* slot;   // slot[0]: the minimum's bits; slot[1]: the block ticket counter
+    double dt_max;
+    double* dt;
+    double* hist;
+    int* err;
 };
 
 __device__ __forceinline__ void fused_cfl_reduce(double best, const FusedCfl& c)
@@ -590,6 +599,18 @@ __device__ __forceinline__ void fused_cfl_reduce(double best, const FusedCfl& c)
         double m = red[0];
         for (int w = 1; w < (int)(blockDim.x >> 5); ++w) m = dmin(m, red[w]);
         atomicMin(c.slot, (unsigned long long)__double_as_longlong(m));
+        __threadfence();
+        const unsigned long long ticket = atomicAdd(c.slot + 1, 1ull);
+        if (ticket == (unsigned long long)gridDim.x - 1) {
+            __threadfence();
+            const double mm = __longlong_as_double((long long)atomicAdd(c.slot, 0ull));
+            const double d = dmin(c.dt_max, mm);
+            c.dt[0] = d;
+            if (c.hist) c.hist[0] = d;
+            if (!(d > 0.0) || !fin(d)) atomicOr(c.err, kErrDt);
+            c.slot[0] = (unsigned long long)__double_as_longlong(HUGE_VAL);
+            c.slot[1] = 0ull;
+        }
     }
 }
 
@@ -902,19 +923,6 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) staged_cd(const doubl
     g_put<NM, D>(b.F, b.cap, t, f);
 }
 
-// dt = min(dt_max, slot) after a fused stage A; re-arms the slot to +inf.
-static __global__ void fused_cfl_finalize(unsigned long long* __restrict__ slot, double dt_max, double* __restrict__ dt,
-                                   double* __restrict__ hist, int* __restrict__ err)
-{
-    pdl_enter();
-    if (blockIdx.x != 0 || threadIdx.x != 0) return;
-    const double m = __longlong_as_double((long long)*slot);
-    const double d = dmin(dt_max, m);
-    dt[0] = d;
-    if (hist) hist[0] = d;
-    if (!(d > 0.0) || !fin(d)) atomicOr(err, kErrDt);
-    *slot = (unsigned long long)__double_as_longlong(HUGE_VAL);
-}
 
 // ---- CFL ------------------------------------------------------------------------
 __device__ __forceinline__ double warp_min(double v)
@@ -1310,14 +1318,10 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         ls.n = n;
         const long long items = (long long)ls.nl * n;
         const unsigned blocks = (unsigned)((items + 255) / 256);
-        FusedCfl fc{0, 0, 0.0, nullptr};
-        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
+        FusedCfl fc{0, 0, 0.0, nullptr, 0.0, nullptr, nullptr, nullptr};
+        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err};
         launch_stage(staged_a<NM, D, DIR>, blocks, s, in, g, M, ls, b, fc);
         count_launches(1);
-        if (fs.on) {
-            launch_stage_dims(fused_cfl_finalize, 1u, 1u, s, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err);
-            count_launches(1);
-        }
         const unsigned blocks2 = (unsigned)((2 * items + 255) / 256);
         launch_stage(staged_bf<NM, D, DIR>, blocks2, s, g, M, ls, b);
         count_launches(1);
@@ -1382,14 +1386,10 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
         ls.n = n;
         const long long items = (long long)ls.nl * n;
         const unsigned blocks = (unsigned)((items + 255) / 256);
-        FusedCfl fc{0, 0, 0.0, nullptr};
-        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot};
+        FusedCfl fc{0, 0, 0.0, nullptr, 0.0, nullptr, nullptr, nullptr};
+        if (fs.on) fc = FusedCfl{1, fs.unsplit, fs.cfl, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err};
         launch_stage(mixed_a<NM, D, DIR>, blocks, s, in, g, M, ls, b, fc);
         count_launches(1);
-        if (fs.on) {
-            launch_stage_dims(fused_cfl_finalize, 1u, 1u, s, fs.slot, fs.dt_max, fs.dt, fs.hist, fs.err);
-            count_launches(1);
-        }
         if (twin) {
             launch_stage(mixed_b<NM, D, DIR, double>, blocks, s, in, g, M, ls, b, dt);
             launch_stage(mixed_cd<NM, D, DIR, double>, blocks, s, in, g, M, ls, b, err);

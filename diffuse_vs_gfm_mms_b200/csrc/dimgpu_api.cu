@@ -452,10 +452,11 @@ cudaError_t alloc_small(dimgpu_session* s)
     if (e == cudaSuccess) e = cudaMalloc(&s->hist, sizeof(double) * kHistCap);
     if (e == cudaSuccess) e = cudaMalloc(&s->partial, sizeof(double) * kTotalsBlocks * (DIMGPU_MAX_MATERIALS + 5));
     if (e == cudaSuccess) e = cudaMalloc(&s->err, sizeof(int));
-    if (e == cudaSuccess) e = cudaMalloc(&s->cfl_slot, sizeof(unsigned long long));
+    // the fused CFL slot (a double's bits, +inf when armed) and its block ticket counter
+    if (e == cudaSuccess) e = cudaMalloc(&s->cfl_slot, 2 * sizeof(unsigned long long));
     if (e == cudaSuccess) {
-        static const double inf = HUGE_VAL;
-        e = cudaMemcpyAsync(s->cfl_slot, &inf, sizeof inf, cudaMemcpyHostToDevice, s->stream);
+        static const unsigned long long armed[2] = {0x7FF0000000000000ull, 0ull};  // +inf's bits, ticket 0
+        e = cudaMemcpyAsync(s->cfl_slot, armed, sizeof armed, cudaMemcpyHostToDevice, s->stream);
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(s->err, 0, sizeof(int), s->stream);
     return e;

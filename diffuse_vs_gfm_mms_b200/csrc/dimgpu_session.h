@@ -29,7 +29,7 @@ struct dimgpu_session {
     dimgpu::Tile tile[3] = {{128, 1}, {64, 4}, {64, 4}};
     int schedule[3] = {DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED, DIMGPU_SCHEDULE_STAGED};
     double* staged = nullptr;  // scratch of the staged schedule (allocated on first use)
-    unsigned long long* cfl_slot = nullptr;  // fused CFL minimum (bit pattern of a double)
+    unsigned long long* cfl_slot = nullptr;  // fused CFL: [0] minimum (a double's bits), [1] block ticket counter
     long long staged_cap = 0;
     std::string msg;
     // profiling
