@@ -71,3 +71,52 @@ def test_long_run_matches_the_reference(case):
             assert bitwise_equal(out[:, idx], rec[f"s{c}_sample"]), f"{case} step {c}: sampled cells differ"
             assert sha256(out) == str(rec[f"s{c}_sha256"]), f"{case} step {c}: state differs from the reference"
     assert bitwise_equal(np.concatenate(dts), rec["dt"])
+
+
+def test_slabs_reproduce_the_long_record():
+    """The slab solver (four slabs of the c1 grid on one GPU, the ghost
+    exchange as device copies) through the shock-bubble interaction: the
+    same hash as the reference at every checkpoint and the same dts."""
+    from diffuse_vs_gfm_mms_b200.dim import Slabs
+
+    case = "c1_shock_bubble_1024x512"
+    path = os.path.join(GOLDEN, f"long_{case}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"{os.path.basename(path)} not generated")
+    rec = np.load(path)
+    d, U = GENERATORS[case]()
+    cfl = float(rec["cfl"])
+    dts = []
+    with Slabs(d, [0, 0, 0, 0], U) as L:
+        done = 0
+        for c in rec["checkpoints"]:
+            c = int(c)
+            dts.append(L.steps(c - done, cfl, 1e300))
+            done = c
+            assert sha256(L.download()) == str(rec[f"s{c}_sha256"]), f"slabs, step {c}"
+    assert bitwise_equal(np.concatenate(dts), rec["dt"])
+
+
+def test_server_solo_lane_reproduces_the_long_record():
+    """A c1 solve submitted to the serving loop (a solo lane: a session shell
+    over the server's arena) beside small batch-lane solves: its 100-step
+    state is the reference's, bit for bit."""
+    from diffuse_vs_gfm_mms_b200 import serve
+
+    case = "c1_shock_bubble_1024x512"
+    path = os.path.join(GOLDEN, f"long_{case}.npz")
+    if not os.path.exists(path):
+        pytest.skip(f"{os.path.basename(path)} not generated")
+    rec = np.load(path)
+    d, U = GENERATORS[case]()
+    n = int(rec["checkpoints"][0])
+    big = serve.Request(rid=0, desc=d, U=U, steps=n, cfl=float(rec["cfl"]), dt_max=1e300, arrival=0.0)
+    small = serve.make_requests(6, rate=0.0, seed=21, steps_range=(20, 60), n1d_range=(64, 512),
+                                side2d_range=(16, 64))
+    for k, r in enumerate(small):
+        r.rid = k + 1
+    with serve.Server(hbm_budget_bytes=8e9, max_slots=16, quantum=8) as srv:
+        stats = srv.serve([big] + small)
+    res = {r.rid: r for r in stats.results}
+    assert sha256(res[0].U) == str(rec[f"s{n}_sha256"])
+    assert bitwise_equal(res[0].dts, rec["dt"][:n])
