@@ -233,3 +233,32 @@ def test_fp32_cost_at_full_size_after_the_interaction():
     assert np.all(np.isfinite(out)) and np.all(np.isfinite(twin))
     bound = REL_L1_TOL if sens.max() <= 1e-7 else max(REL_L1_TOL, 10.0 * sens.max())
     assert np.all(fp32 <= bound), (fp32, sens)
+
+
+def test_fp32_cost_on_the_cloud_at_128cubed():
+    """c2's generator at 128^3 (64 bubbles in stiffened water) over 100
+    steps: mixed against its FP64 twin, bounded by the twin's own 1e-15
+    response, and the twin against the reference's 100-step record on its
+    sampled cells."""
+    import os
+
+    from helpers import GOLDEN
+
+    d, U = W.bubble_cloud_3d(N=(128, 128, 128))
+    n = 100
+    out, dts = _mixed(d, U, 0.6, n)
+    twin, tdts = _twin(d, U, 0.6, n)
+    rng = np.random.default_rng(11)
+    tp, _ = _twin(d, U * (1.0 + 1e-15 * rng.standard_normal(U.shape)), 0.6, n)
+    fp32 = _report("c2 cloud 128^3, 100 steps — mixed vs FP64 twin", out, twin, dts, tdts, d)
+    sens = _rel_l1_scored(tp, twin, d)
+    print(f"  twin moved by a 1e-15 input perturbation: rel L1 {_fmt(sens)}")
+    path = os.path.join(GOLDEN, "long_c2_cloud_128cubed.npz")
+    if os.path.exists(path):
+        rec = np.load(path)
+        idx = rec["sample_index"]
+        _report("c2 cloud 128^3, 100 steps — FP64 twin vs the reference (sampled cells)", twin[:, idx],
+                rec[f"s{n}_sample"], tdts, rec["dt"][:n], d)
+    assert np.all(np.isfinite(out)) and np.all(np.isfinite(twin))
+    bound = REL_L1_TOL if sens.max() <= 1e-7 else max(REL_L1_TOL, 10.0 * sens.max())
+    assert np.all(fp32 <= bound), (fp32, sens)
