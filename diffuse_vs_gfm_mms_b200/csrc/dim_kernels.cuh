@@ -778,6 +778,109 @@ __global__ void __launch_bounds__(256, DIMGPU_E_MINB) staged_e(const double* __r
     store_cell<NM, D>(out, g.ncell, it.cell, Un);
 }
 
+// Stages D and E in one kernel.  A block owns a tile of TW lines x TH
+// positions along them: every position gi >= 1 forms the face gi-1|gi
+// (stage D of item gi-1) into shared memory, then the tile's first TH - 1
+// positions update their cells from the faces on either side (stage E).
+// Consecutive tiles along a line overlap by one position, so a face is
+// formed twice only at tile seams (1 face in TH - 1).  The face records
+// never reach HBM.  The x sweep puts the positions on the fast thread index
+// (neighbouring items t and t+1), the other axes put the lines there.
+template<int DIR>
+struct DeTile {
+    static constexpr int TW = DIR == 0 ? 8 : 16;   // lines per tile
+    static constexpr int TH = DIR == 0 ? 32 : 16;  // positions per tile (TH - 1 cells updated)
+};
+
+template<int NM, int D, int DIR>
+__host__ __device__ inline long long de_tiles_per_line(int n)
+{
+    return (n + DeTile<DIR>::TH - 2) / (DeTile<DIR>::TH - 1);
+}
+
+template<int NM, int D, int DIR>
+__global__ void __launch_bounds__(256, DIMGPU_DE_MINB) staged_de(const double* __restrict__ in, double* __restrict__ out,
+                                                 __grid_constant__ const Grid g, __grid_constant__ const Mats M, LineSet ls,
+                                                 StagedBufs<NM, D> b, const double* __restrict__ dtp,
+                                                 int* __restrict__ err)
+{
+    constexpr int TW = DeTile<DIR>::TW, TH = DeTile<DIR>::TH, KF = kFaceVars(NM, D);
+    static_assert(TW * TH == 256, "one thread per tile position");
+    __shared__ double sf[KF][256];
+    pdl_enter();
+    const int tx = threadIdx.x;
+    const int lo_ = DIR == 0 ? tx / TH : tx % TW;  // line within the tile
+    const int po = DIR == 0 ? tx % TH : tx / TW;   // position within the tile
+    const long long tpl = de_tiles_per_line<NM, D, DIR>(ls.n);
+    const long long lrel = (long long)(blockIdx.x / tpl) * TW + lo_;
+    const int gi = (int)(blockIdx.x % tpl) * (TH - 1) + po;
+    const int n = ls.n;
+    const bool live = lrel < ls.nl && gi < n;
+    const long long t = DIR == 0 ? lrel * n + gi : (long long)gi * ls.nl + lrel;
+
+    // Stage D: the face to the left of position gi (item gi-1's face).
+    if (live && gi >= 1) {
+        const long long s = DIR == 0 ? 1 : ls.nl;
+        State<NM, D> UL, UR;
+        Prim<NM, D> PL, PR;
+        g_get<NM, D>(b.RS, b.cap, t - s, UL);
+        g_get<NM, D>(b.PRS, b.cap, t - s, PL);
+        g_get<NM, D>(b.LS, b.cap, t, UR);
+        g_get<NM, D>(b.PLS, b.cap, t, PR);
+        FaceD<NM, D> f;
+        if (!stage_d<NM, D, DIMGPU_STAGED_INLINE_DE>(M, UL, PL, UR, PR, DIR, f)) atomicOr(err, kErrNonFinite);
+        int v = 0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) sf[v++][tx] = f.F.m[k];
+#pragma unroll
+        for (int d = 0; d < D; ++d) sf[v++][tx] = f.F.mom[d];
+        sf[v++][tx] = f.F.E;
+        sf[v++][tx] = f.fv;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) sf[v++][tx] = f.af[k];
+    }
+    __syncthreads();
+
+    // Stage E on the tile's first TH - 1 positions.
+    if (!live || po == TH - 1) return;
+    const StagedItem<DIR> it(g, ls, t);
+    const bool first = gi == 0, last = gi == n - 1;
+    State<NM, D> U;
+    load_cell<NM, D>(in, g.ncell, it.cell, U);
+    CellA<NM, D> A;
+    g_get<NM, D>(b.P, b.cap, t, A.P);
+#pragma unroll
+    for (int k = 0; k < NM; ++k) A.ck[k] = b.ck[k * b.cap + t];
+    FaceD<NM, D> fl, fh;
+    const int th = tx + (DIR == 0 ? 1 : TW);  // the next position's thread
+    if (!first) {
+        int v = 0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) fl.F.m[k] = sf[v++][tx];
+#pragma unroll
+        for (int d = 0; d < D; ++d) fl.F.mom[d] = sf[v++][tx];
+        fl.F.E = sf[v++][tx];
+        fl.fv = sf[v++][tx];
+#pragma unroll
+        for (int k = 0; k < NM; ++k) fl.af[k] = sf[v++][tx];
+    }
+    if (!last) {
+        int v = 0;
+#pragma unroll
+        for (int k = 0; k < NM; ++k) fh.F.m[k] = sf[v++][th];
+#pragma unroll
+        for (int d = 0; d < D; ++d) fh.F.mom[d] = sf[v++][th];
+        fh.F.E = sf[v++][th];
+        fh.fv = sf[v++][th];
+#pragma unroll
+        for (int k = 0; k < NM; ++k) fh.af[k] = sf[v++][th];
+    }
+    State<NM, D> Un;
+    stage_e<NM, D, DIMGPU_STAGED_INLINE_DE>(M, U, A, first ? nullptr : &fl, last ? nullptr : &fh, first, last, *dtp,
+                                             g.dx[DIR], Un);
+    store_cell<NM, D>(out, g.ncell, it.cell, Un);
+}
+
 // ---- the mixed-precision staged sweep (precision MIXED) ---------------------------
 //
 // Stage A is mixed_a (staged_a with the closed-form FP64 recovery), stage E
@@ -1327,6 +1430,7 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         count_launches(1);
         launch_stage(staged_bu<NM, D, DIR>, blocks, s, in, g, M, ls, b, dt);
         count_launches(1);
+        constexpr bool fuse_de = DIMGPU_STAGED_FUSE_DE && D >= 2 && !DIMGPU_STAGED_FUSE_CD;
         if (DIMGPU_STAGED_FUSE_CD) {
             launch_stage(staged_cd<NM, D, DIR>, blocks, s, in, g, M, ls, b, err);
             count_launches(1);
@@ -1334,10 +1438,19 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         else {
             launch_stage(staged_c<NM, D, DIR>, blocks2, s, in, g, M, ls, b);
             count_launches(1);
-            launch_stage(staged_d<NM, D, DIR>, blocks, s, g, M, ls, b, err);
-            count_launches(1);
+            if constexpr (!fuse_de) {
+                launch_stage(staged_d<NM, D, DIR>, blocks, s, g, M, ls, b, err);
+                count_launches(1);
+            }
         }
-        launch_stage(staged_e<NM, D, DIR>, blocks, s, in, out, g, M, ls, b, dt);
+        if constexpr (fuse_de) {
+            const long long tiles =
+                ((ls.nl + DeTile<DIR>::TW - 1) / DeTile<DIR>::TW) * de_tiles_per_line<NM, D, DIR>(n);
+            launch_stage(staged_de<NM, D, DIR>, (unsigned)tiles, s, in, out, g, M, ls, b, dt, err);
+        }
+        else {
+            launch_stage(staged_e<NM, D, DIR>, blocks, s, in, out, g, M, ls, b, dt);
+        }
         count_launches(1);
         const cudaError_t e = cudaGetLastError();
         if (e != cudaSuccess) return e;

@@ -115,6 +115,19 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_FUSE_CD false
 #endif
 
+// Whether the staged schedule of a 2D or 3D grid runs stages D and E as one
+// kernel (staged_de: a tile's faces handed to its cells through shared
+// memory) instead of staged_d + staged_e.  Measured on a B200: c1 0.601
+// against 0.590 ms per step, c2 at 512^3 230.9 against 220.9 ms (the fused
+// kernel spills at 80 registers, 0.617 ms at 2 blocks per SM, and its
+// cells wait at the barrier for the tile's slowest face), so off.
+#ifndef DIMGPU_STAGED_FUSE_DE
+#define DIMGPU_STAGED_FUSE_DE false
+#endif
+#ifndef DIMGPU_DE_MINB
+#define DIMGPU_DE_MINB DIMGPU_STAGED_MINB
+#endif
+
 // Whether the staged D and E kernels inline their sound speeds and repairs
 // (two call sites each) instead of calling the out-of-line copies.
 // Measured on a B200: 1.5 % less time per step on c1 and c2 inlined.
