@@ -30,7 +30,7 @@ FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC",
 SOURCES = ["inst_nm1.cu", "inst_nm2.cu", "inst_nm3.cu", "inst_nm4.cu", "inst_euler.cu", "dimgpu_api.cu",
            "dimgpu_noalloc.cu", "dimgpu_batch.cu", "dimgpu_io.cu", "dimgpu_server.cu", "dimgpu_slabs.cu"]
 HEADERS = ["dim_physics.h", "dim_line.h", "dim_kernels.cuh", "dim_launch.h", "dim_batch.cuh", "dim_mixed.h",
-           "dimgpu_validate.h", "dimgpu_session.h", "dim_io.cuh", "range_alloc.h", "pdl.cuh",
+           "dimgpu_validate.h", "dimgpu_session.h", "dim_io.cuh", "range_alloc.h", "pdl.cuh", "fastdiv.h",
            "euler_physics.h", "euler_kernels.cuh"]
 
 

@@ -13,6 +13,7 @@
 
 #include "dim_launch.h"
 #include "pdl.cuh"
+#include "fastdiv.h"
 #include "dim_line.h"
 #include "dim_mixed.h"
 #include "dimgpu.h"
@@ -402,6 +403,17 @@ struct LineSet {
     long long L0;  // first line of the chunk
     int nl;        // lines in the chunk
     int n;         // cells per line
+    // Dividers by n, nl and the grid's N[0], set by set_dividers() on the
+    // host for the staged kernels (item and line indices stay below 2^32:
+    // a chunk holds at most max(2^24, longest line) cells, and a grid's
+    // line count is bounded by HBM far below 2^32).
+    FastDiv by_n, by_nl, by_n0;
+    __host__ void set_dividers(int n0)
+    {
+        by_n.set((unsigned)n);
+        by_nl.set((unsigned)nl);
+        by_n0.set((unsigned)n0);
+    }
 };
 
 template<int NM, int D>
@@ -546,7 +558,10 @@ __device__ __forceinline__ void g_get(const double* b, long long cap, long long 
 
 // Item t of a chunk: its cell index along the line, its cell in the grid and
 // the scratch stride between neighbours along the line.
-template<int DIR>
+// FD: divide through the LineSet's dividers (the staged kernels, whose
+// LineSet the host fills) instead of 64-bit integer division (the batch
+// kernels, which build theirs on the device).
+template<int DIR, bool FD = DIMGPU_STAGED_FASTDIV>
 struct StagedItem {
     int gi;
     long long cell;
@@ -554,13 +569,39 @@ struct StagedItem {
     __device__ __forceinline__ StagedItem(const Grid& g, const LineSet& ls, long long t)
     {
         long long lrel;
-        if (DIR == 0) { lrel = t / ls.n; gi = (int)(t % ls.n); s = 1; }
+        if (FD) {
+            const unsigned u = (unsigned)t;
+            if (DIR == 0) {
+                const unsigned q = ls.by_n.div(u);
+                lrel = q;
+                gi = (int)(u - q * (unsigned)ls.n);
+                s = 1;
+            }
+            else {
+                const unsigned q = ls.by_nl.div(u);
+                gi = (int)q;
+                lrel = u - q * (unsigned)ls.nl;
+                s = ls.nl;
+            }
+        }
+        else if (DIR == 0) { lrel = t / ls.n; gi = (int)(t % ls.n); s = 1; }
         else { gi = (int)(t / ls.nl); lrel = t % ls.nl; s = ls.nl; }
         const long long L = ls.L0 + lrel;
         long long base;
         if (DIR == 0) base = L * g.N[0];
-        else if (DIR == 1) base = (L % g.N[0]) + (L / g.N[0]) * g.stride[2];
-        else base = (L % g.N[0]) + (L / g.N[0]) * g.stride[1];
+        else {
+            long long lx, ly;
+            if (FD) {
+                const unsigned q = ls.by_n0.div((unsigned)L);
+                ly = q;
+                lx = (unsigned)L - q * (unsigned)g.N[0];
+            }
+            else {
+                lx = L % g.N[0];
+                ly = L / g.N[0];
+            }
+            base = lx + ly * g.stride[DIR == 1 ? 2 : 1];
+        }
         cell = base + (long long)gi * g.stride[DIR];
     }
 };
@@ -945,9 +986,9 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_BCD_MINB) mixed_b(const doub
 }
 
 // Face state of cell item t on the given side (end cells: U and P).
-template<int NM, int D, int DIR, typename R = float>
+template<int NM, int D, int DIR, typename R = float, bool FD = DIMGPU_STAGED_FASTDIV>
 __device__ __forceinline__ void mixed_face(const double* __restrict__ in, const Grid& g, const Mats& M,
-                                           const StagedBufs<NM, D>& b, const StagedItem<DIR>& it, long long t, int n,
+                                           const StagedBufs<NM, D>& b, const StagedItem<DIR, FD>& it, long long t, int n,
                                            bool right, State<NM, D>& Uf, Prim<NM, D>& Pf)
 {
     const bool end = it.gi == 0 || it.gi == n - 1 || n < 3;
@@ -1401,7 +1442,7 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
     const int n = g.N[DIR];
     const long long nlines = g.ncell / n;
     long long per = cap / n;
-    if (per < 1) return cudaErrorInvalidValue;
+    if (per < 1 || nlines > 0xFFFFFFFFLL || 2 * cap > 0xFFFFFFFFLL) return cudaErrorInvalidValue;
     StagedBufs<NM, D> b;
     b.cap = cap;
     double* p = scratch;
@@ -1419,6 +1460,7 @@ cudaError_t launch_staged_dir(const Grid& g, const Mats& M, const double* in, do
         ls.L0 = L0;
         ls.nl = (int)((nlines - L0 < per) ? (nlines - L0) : per);
         ls.n = n;
+        ls.set_dividers(g.N[0]);
         const long long items = (long long)ls.nl * n;
         const unsigned blocks = (unsigned)((items + 255) / 256);
         FusedCfl fc{0, 0, 0.0, nullptr, 0.0, nullptr, nullptr, nullptr};
@@ -1481,7 +1523,7 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
     const int n = g.N[DIR];
     const long long nlines = g.ncell / n;
     const long long per = cap / n;
-    if (per < 1) return cudaErrorInvalidValue;
+    if (per < 1 || nlines > 0xFFFFFFFFLL || 2 * cap > 0xFFFFFFFFLL) return cudaErrorInvalidValue;
     StagedBufs<NM, D> b;
     b.cap = cap;
     double* p = scratch;
@@ -1497,6 +1539,7 @@ cudaError_t launch_mixed_dir(const Grid& g, const Mats& M, const double* in, dou
         ls.L0 = L0;
         ls.nl = (int)((nlines - L0 < per) ? (nlines - L0) : per);
         ls.n = n;
+        ls.set_dividers(g.N[0]);
         const long long items = (long long)ls.nl * n;
         const unsigned blocks = (unsigned)((items + 255) / 256);
         FusedCfl fc{0, 0, 0.0, nullptr, 0.0, nullptr, nullptr, nullptr};

@@ -115,6 +115,13 @@ struct dimgpu_batch;
 #define DIMGPU_STAGED_FUSE_CD false
 #endif
 
+// Whether the staged kernels split their item index into line and position
+// with precomputed multiply-high dividers (FastDiv) instead of 64-bit
+// integer division.
+#ifndef DIMGPU_STAGED_FASTDIV
+#define DIMGPU_STAGED_FASTDIV true
+#endif
+
 // Whether the staged schedule of a 2D or 3D grid runs stages D and E as one
 // kernel (staged_de: a tile's faces handed to its cells through shared
 // memory) instead of staged_d + staged_e.  Measured on a B200: c1 0.601

@@ -36,7 +36,7 @@ def build_host_harness() -> str:
     src = os.path.join(ROOT, "tests", "native", "physics_host.cpp")
     csrc = os.path.join(ROOT, "diffuse_vs_gfm_mms_b200", "csrc")
     deps = [src] + [os.path.join(csrc, h) for h in ("dim_physics.h", "dim_line.h", "dim_mixed.h",
-                                                                "euler_physics.h")]
+                                                                "euler_physics.h", "fastdiv.h")]
     if os.path.exists(HOST_SO) and os.path.getmtime(HOST_SO) >= max(os.path.getmtime(p) for p in deps):
         return HOST_SO
     os.makedirs(os.path.dirname(HOST_SO), exist_ok=True)

@@ -15,6 +15,7 @@ static long long g_opcount[16];
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_line.h"
 #include "../../diffuse_vs_gfm_mms_b200/csrc/dim_mixed.h"
 #include "../../diffuse_vs_gfm_mms_b200/csrc/euler_physics.h"
+#include "../../diffuse_vs_gfm_mms_b200/csrc/fastdiv.h"
 #include "dimgpu.h"
 
 using namespace dimgpu;
@@ -461,6 +462,19 @@ int host_euler_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, cons
 int host_sweep_direction(const dimgpu_desc* d, int dir, double dt, const double* in, double* out)
 {
     DISPATCH(d, sweep_impl, d, dir, dt, in, out);
+}
+
+// q[i] = x[i] / d and r[i] = x[i] % d through the staged kernels' FastDiv.
+int host_fastdiv(unsigned d, int n, const unsigned* x, unsigned* q, unsigned* r)
+{
+    if (d == 0) return DIMGPU_E_INVALID_ARG;
+    dimgpu::FastDiv f;
+    f.set(d);
+    for (int i = 0; i < n; ++i) {
+        q[i] = f.div(x[i]);
+        r[i] = x[i] - q[i] * d;
+    }
+    return DIMGPU_OK;
 }
 
 // Copies the operation counts into out[0 .. n) and, if reset, zeroes them.

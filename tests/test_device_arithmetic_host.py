@@ -143,3 +143,35 @@ def test_sweep_stages_against_oracle(host, port, name, gen):
     dt = port.compute_dt_cfl(d, U, 0.8, 1e300)
     for direction in range(d.dim):
         assert ndiff(host.sweep_direction(d, direction, dt, U), port.sweep_direction(d, direction, dt, U)) == 0
+
+
+def _divisors():
+    rng = np.random.default_rng(7)
+    ds = {1, 2, 3, 5, 6, 7, 31, 518, 1030, 1024, 2048, (1 << 24) + 3, (1 << 31) - 1, 1 << 31,
+          (1 << 31) + 1, (1 << 32) - 1}
+    ds |= {(1 << k) + e for k in range(1, 32) for e in (-1, 0, 1) if 1 <= (1 << k) + e < (1 << 32)}
+    ds |= set(int(v) for v in rng.integers(1, 1 << 32, 200, dtype=np.uint64))
+    ds |= set(int(v) for v in rng.integers(1, 5000, 200))
+    return sorted(ds)
+
+
+def test_fastdiv_divides_every_index_exactly(host):
+    """The staged kernels split item and line indices with FastDiv
+    (csrc/fastdiv.h): quotient and remainder equal integer division for
+    divisors over the whole 32-bit range and dividends at 0, 2^32 - 1, near
+    multiples of the divisor and at random."""
+    rng = np.random.default_rng(11)
+    f = host.lib.host_fastdiv
+    f.argtypes = [C.c_uint, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p]
+    for d in _divisors():
+        k = rng.integers(0, (1 << 32) // d, 64, dtype=np.uint64)
+        near = np.concatenate([k * d, k * d + d - 1, k * d - 1, k * d + 1])
+        x = np.concatenate([near, rng.integers(0, 1 << 32, 2048, dtype=np.uint64),
+                            np.array([0, 1, d - 1, d, (1 << 32) - 1], dtype=np.uint64)])
+        x = x[x < (1 << 32)].astype(np.uint32)
+        q = np.empty_like(x)
+        r = np.empty_like(x)
+        assert f(d, x.size, x.ctypes.data, q.ctypes.data, r.ctypes.data) == 0
+        xx = x.astype(np.uint64)
+        assert np.array_equal(q.astype(np.uint64), xx // d), d
+        assert np.array_equal(r.astype(np.uint64), xx % d), d
