@@ -189,6 +189,45 @@ def test_large_3d_lines_match_oracle(port):
         assert np.all(np.isfinite(cur))
 
 
+def test_multi_chunk_3d_lines_match_oracle(port):
+    """A grid above one scratch chunk (2^24 cells): 256 x 256 x 260, so each
+    axis runs as two chunks of whole lines and the second chunk's items
+    index lines from L0 > 0.  Lines on both sides of every chunk seam, the
+    last line and random lines of each chunk against the oracle's
+    solve_line."""
+    N = (256, 256, 260)
+    d, U = W.bubble_cloud_3d(N=N, nbubbles=64)
+    rng = np.random.default_rng(1)
+    V = d.nvar
+    nlines = [N[1] * N[2], N[0] * N[2], N[0] * N[1]]
+    with Session(d, U) as s:
+        dt = s.compute_dt_cfl(0.6, 1e300)
+        cur = U.reshape(V, N[2], N[1], N[0])
+        for direction in range(3):
+            s.sweep_direction(direction, dt)
+            new = s.download().reshape(V, N[2], N[1], N[0])
+            per = (1 << 24) // N[direction]
+            assert per < nlines[direction]
+            picks = [0, per - 1, per, per + 1, nlines[direction] - 1]
+            picks += list(rng.integers(0, per, 6)) + list(rng.integers(per, nlines[direction], 6))
+            for L in picks:
+                L = int(L)
+                if direction == 0:
+                    z, y = divmod(L, N[1])
+                    line_in, line_out = cur[:, z, y, :], new[:, z, y, :]
+                elif direction == 1:
+                    z, x = divmod(L, N[0])
+                    line_in, line_out = cur[:, z, :, x], new[:, z, :, x]
+                else:
+                    y, x = divmod(L, N[0])
+                    line_in, line_out = cur[:, :, y, x], new[:, :, y, x]
+                ref = port.solve_line(d, direction, dt, d.dx[direction], line_in.T.copy())
+                assert ndiff(line_out.T, ref) == 0, (direction, L)
+            s.apply_boundary_conditions()
+            cur = s.download().reshape(V, N[2], N[1], N[0])
+        assert np.all(np.isfinite(cur))
+
+
 def test_repeatable():
     d, U = W.shock_bubble_2d(N=(256, 128))
     res = []
