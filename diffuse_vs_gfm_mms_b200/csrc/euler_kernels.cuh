@@ -15,6 +15,7 @@
 
 #include "dim_launch.h"
 #include "pdl.cuh"
+#include "fastdiv.h"
 #include "euler_physics.h"
 #include "dimgpu.h"
 
@@ -101,11 +102,19 @@ __device__ __forceinline__ void e_get(const double* sm, int NT, int t, EPrim<D>&
 // Launch bound: 4 blocks of 256 threads per SM (64 registers a thread).  The
 // sweep is latency-bound on dependent FP64 chains; the extra warps hide more
 // of that latency than the few spilled registers (L1-resident) cost.
+// Launch-invariant dividers of the tile mapping (thread -> position and
+// line in the tile, block -> tile and line group), set on the host, and
+// the grid's line count along x.
+struct EulerTileDiv {
+    FastDiv by_T, by_W, by_ntile, by_ngx;
+    long long nlines;
+};
+
 template<int D, int DIR>
 __global__ void __launch_bounds__(256, DIMGPU_EULER_MINB) euler_sweep_kernel(const double* __restrict__ in, double* __restrict__ out,
                                                              __grid_constant__ const Grid g, __grid_constant__ const Mats M, int T, int W, int ntile, int ngx,
-                                                             const double* __restrict__ dtp, int* __restrict__ err,
-                                                             int ends_copy)
+                                                             EulerTileDiv dv, const double* __restrict__ dtp,
+                                                             int* __restrict__ err, int ends_copy)
 {
     pdl_enter();
     extern __shared__ double sm[];
@@ -118,25 +127,27 @@ __global__ void __launch_bounds__(256, DIMGPU_EULER_MINB) euler_sweep_kernel(con
     const int OUT = T - 6;
 
     int pos, j, s;
-    if (DIR == 0) { pos = t % T; j = t / T; s = 1; }
-    else { j = t % W; pos = t / W; s = W; }
+    if (DIR == 0) { j = (int)dv.by_T.div((unsigned)t); pos = t - j * T; s = 1; }
+    else { pos = (int)dv.by_W.div((unsigned)t); j = t - pos * W; s = W; }
 
-    const long long bid = blockIdx.x;
+    const unsigned bid = blockIdx.x;
     int tile;
     long long base, sline;
     bool line_ok;
     if (DIR == 0) {
-        tile = (int)(bid % ntile);
-        const long long L = (bid / ntile) * W + j;
-        line_ok = L < g.ncell / g.N[0];
+        const unsigned q = dv.by_ntile.div(bid);
+        tile = (int)(bid - q * (unsigned)ntile);
+        const long long L = (long long)q * W + j;
+        line_ok = L < dv.nlines;
         base = L * g.N[0];
         sline = 1;
     }
     else {
-        const int gx = (int)(bid % ngx);
-        const long long rest = bid / ngx;
-        tile = (int)(rest % ntile);
-        const long long other = rest / ntile;
+        const unsigned rest = dv.by_ngx.div(bid);
+        const int gx = (int)(bid - rest * (unsigned)ngx);
+        const unsigned other_u = dv.by_ntile.div(rest);
+        tile = (int)(rest - other_u * (unsigned)ntile);
+        const long long other = other_u;
         const int x = gx * W + j;
         line_ok = x < g.N[0];
         base = (DIR == 1) ? x + other * g.stride[2] : x + other * g.stride[1];
@@ -492,8 +503,15 @@ cudaError_t launch_euler_sweep_dir(const Grid& g, const Mats& M, Tile tile, cons
     auto kern = euler_sweep_kernel<D, DIR>;
     const cudaError_t ea = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (ea != cudaSuccess) return ea;
-    launch_stage_smem(kern, (unsigned)nblocks, (unsigned)(T * W), smem, s, in, out, g, M, T, W, ntile, ngx, dt, err,
-                      ends_copy);
+    if (nblocks > 0xFFFFFFFFLL) return cudaErrorInvalidValue;
+    EulerTileDiv dv;
+    dv.by_T.set((unsigned)T);
+    dv.by_W.set((unsigned)W);
+    dv.by_ntile.set((unsigned)ntile);
+    dv.by_ngx.set((unsigned)ngx);
+    dv.nlines = g.ncell / g.N[0];
+    launch_stage_smem(kern, (unsigned)nblocks, (unsigned)(T * W), smem, s, in, out, g, M, T, W, ntile, ngx, dv, dt,
+                      err, ends_copy);
     count_launches(1);
     return cudaGetLastError();
 }
