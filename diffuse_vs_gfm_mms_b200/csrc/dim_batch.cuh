@@ -123,8 +123,11 @@ __global__ void __launch_bounds__(256) batch_finalize(BInst* __restrict__ tab, c
         LineSet ls;                                                                        \
         ls.L0 = 0;                                                                         \
         ls.n = n;                                                                          \
-        ls.nl = (int)(I.g.ncell / n);                                                      \
-        const StagedItem<DIR, false> it(I.g, ls, t);                                            \
+        ls.nl = I.nl[DIR];                                                                 \
+        ls.by_n = I.by_n[DIR];                                                             \
+        ls.by_nl = I.by_nl[DIR];                                                           \
+        ls.by_n0 = I.by_n0;                                                                \
+        const StagedItem<DIR, DIMGPU_STAGED_FASTDIV> it(I.g, ls, t);                       \
         const long long q = I.soff + t;                                                    \
         const double* in = I.st[I.cur ^ rel];                                              \
         (void)in;
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(256, DIMGPU_STAGED_MINB) batch_d(const BInst* 
     if (I.mixed) {
         // mixed_cd: both face states from the half-step primitives
         mixed_face<NM, D, DIR>(in, I.g, I.M, b, it, q, n, true, UL, PL);
-        StagedItem<DIR, false> nx = it;
+        StagedItem<DIR, DIMGPU_STAGED_FASTDIV> nx = it;
         nx.gi += 1;
         nx.cell += I.g.stride[DIR];
         mixed_face<NM, D, DIR>(in, I.g, I.M, b, nx, q + it.s, n, false, UR, PR);

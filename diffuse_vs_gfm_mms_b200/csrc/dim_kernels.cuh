@@ -403,10 +403,10 @@ struct LineSet {
     long long L0;  // first line of the chunk
     int nl;        // lines in the chunk
     int n;         // cells per line
-    // Dividers by n, nl and the grid's N[0], set by set_dividers() on the
-    // host for the staged kernels (item and line indices stay below 2^32:
-    // a chunk holds at most max(2^24, longest line) cells, and a grid's
-    // line count is bounded by HBM far below 2^32).
+    // Dividers by n, nl and the grid's N[0], set on the host (item and line
+    // indices stay below 2^32: a chunk holds at most max(2^24, longest
+    // line) cells, a batch instance at most 2^31 - 1, and a grid's line
+    // count is bounded by HBM far below 2^32).
     FastDiv by_n, by_nl, by_n0;
     __host__ void set_dividers(int n0)
     {
@@ -558,9 +558,9 @@ __device__ __forceinline__ void g_get(const double* b, long long cap, long long 
 
 // Item t of a chunk: its cell index along the line, its cell in the grid and
 // the scratch stride between neighbours along the line.
-// FD: divide through the LineSet's dividers (the staged kernels, whose
-// LineSet the host fills) instead of 64-bit integer division (the batch
-// kernels, which build theirs on the device).
+// FD: divide through the LineSet's dividers (set on the host: per chunk for
+// a session's kernels, per instance in the batch's instance table) instead
+// of 64-bit integer division.
 template<int DIR, bool FD = DIMGPU_STAGED_FASTDIV>
 struct StagedItem {
     int gi;

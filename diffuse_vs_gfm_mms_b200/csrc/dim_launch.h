@@ -8,6 +8,7 @@
 #include <string>
 
 #include "dim_physics.h"
+#include "fastdiv.h"
 
 struct dimgpu_batch;
 
@@ -255,6 +256,8 @@ struct BInst {
     int mixed;          // DIMGPU_PRECISION_MIXED: mixed_b / mixed_cd arithmetic
     double cfl, dt_max;
     double dt;          // dt of the current step
+    int nl[3];          // lines along each axis (ncell / N[a])
+    FastDiv by_n[3], by_nl[3], by_n0;  // dividers of the staged item index (set on the host)
 };
 
 // Device tables and scratch of one batched step.

@@ -416,6 +416,7 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
         if (a < d->dim && (d->N[a] == 2 || d->N[a] == 3))
             return bfail(b, DIMGPU_E_UNSUPPORTED, "the batch needs N = 1 or N >= 4 on every axis");
         ncell *= d->N[a];
+        if (ncell > 0x7FFFFFFFLL) return bfail(b, DIMGPU_E_INVALID_ARG, "an instance holds at most 2^31 - 1 cells");
     }
     for (int k = 0; k < d->nmat; ++k) {
         if (d->mat[k].kind != DIMGPU_EOS_IDEAL_GAS && d->mat[k].kind != DIMGPU_EOS_STIFFENED_GAS)
@@ -454,6 +455,12 @@ int dimgpu_batch_add(dimgpu_batch* b, const dimgpu_desc* d, const double* soa, i
     I.g.stride[0] = 1;
     I.g.stride[1] = d->N[0];
     I.g.stride[2] = (long long)d->N[0] * d->N[1];
+    for (int a = 0; a < 3; ++a) {
+        I.nl[a] = (int)(ncell / d->N[a]);
+        I.by_n[a].set((unsigned)d->N[a]);
+        I.by_nl[a].set((unsigned)I.nl[a]);
+    }
+    I.by_n0.set((unsigned)d->N[0]);
     I.steps_left = steps;
     I.mixed = d->precision == DIMGPU_PRECISION_MIXED ? 1 : 0;
     I.cfl = cfl;
