@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(256, DIMGPU_A_MINB) staged_a(const double* __r
         if (!DIMGPU_STAGED_NO_PE) g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
-        if (fc.on) best = cfl_candidate<NM, D, true>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+        if (fc.on) best = cfl_candidate<NM, D, true>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0, A.ck);
     }
     if (fc.on) fused_cfl_reduce(best, fc);
 }
@@ -947,7 +947,7 @@ __global__ void __launch_bounds__(256, DIMGPU_MIXED_A_MINB) mixed_a(const double
         if (!DIMGPU_STAGED_NO_PE) g_put<NM, D>(b.Pe, b.cap, t, A.Pe);
 #pragma unroll
         for (int k = 0; k < NM; ++k) b.ck[k * b.cap + t] = A.ck[k];
-        if (fc.on) best = cfl_candidate<NM, D, DIMGPU_MIXED_INLINE>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0);
+        if (fc.on) best = cfl_candidate<NM, D, DIMGPU_MIXED_INLINE>(M, U, A.P, g.dx, fc.cfl, fc.unsplit != 0, A.ck);
     }
     if (fc.on) fused_cfl_reduce(best, fc);
 }

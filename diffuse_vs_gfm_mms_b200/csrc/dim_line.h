@@ -52,10 +52,13 @@ DHD State<NM, D> repair(const Mats& M, const State<NM, D>& U)
     else return repair_state_v<NM, D>(M, U);
 }
 
+// ck (inlined form only): material sound speeds of the same primitive to
+// reuse where their arguments agree, or nullptr.
 template<int NM, bool IL>
-DHD double sound(const Mats& M, double rho_total, double p, const double* alpha, const double* rho)
+DHD double sound(const Mats& M, double rho_total, double p, const double* alpha, const double* rho,
+                 const double* ck = nullptr)
 {
-    if constexpr (IL) return sound_speed_generic<NM>(M, rho_total, p, mix_of<NM>(alpha, rho));
+    if constexpr (IL) return sound_speed_generic<NM>(M, rho_total, p, mix_of<NM>(alpha, rho), ck);
     else return generic_mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
 }
 
@@ -244,12 +247,13 @@ DHD void stage_e(const Mats& M, const State<NM, D>& U, const CellA<NM, D>& A, co
 // CFL candidate of one cell (dim::compute_dt_cfl body, src/dim/solver/cfl.hpp:
 // 46-62, and the unsplit variant :94-115): the smallest cfl*dx_d/wave_speed
 // over the axes (or cfl/spectral_sum); +inf when no axis contributes.
-// P = cons_to_prim(U).
+// P = cons_to_prim(U); ck: rhs_sound_speeds of P (stage A has them), or
+// nullptr.
 template<int NM, int D, bool IL = false>
 DHD double cfl_candidate(const Mats& M, const State<NM, D>& U, const Prim<NM, D>& P, const double* dx,
-                         double cfl, bool unsplit)
+                         double cfl, bool unsplit, const double* ck = nullptr)
 {
-    const double c = sound<NM, IL>(M, total_density<NM, D>(U), P.p, P.alpha, P.rho);
+    const double c = sound<NM, IL>(M, total_density<NM, D>(U), P.p, P.alpha, P.rho, ck);
     double best = HUGE_VAL;
     if (unsplit) {
         double spectral_sum = 0.0;

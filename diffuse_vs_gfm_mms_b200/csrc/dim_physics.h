@@ -425,38 +425,55 @@ DHD double pressure_from_internal_energy(const Mats& M, double rho_total, double
     return pressure_from_internal_energy_v<NM>(M, rho_total, e, mix_of<NM>(alpha, rho));
 }
 
+// material_sound_speed(M, k, clamp_min(rho_raw), p_arg), taken from ck[k]
+// where the caller already evaluated it on the same arguments: ck from
+// rhs_sound_speeds of the same primitive, which passes max(finite_or(x),
+// 1e-12) for rho_k and p, and clamp_min leaves x itself as well when x is
+// finite and at least 1e-10 (p_ok: the raw pressure is; p_arg is then the
+// raw pressure, clamped or not).  ck == nullptr: always evaluated.
+DHD double material_speed_or(const Mats& M, int k, double rho_raw, double p_arg, bool p_ok, const double* ck)
+{
+    if (ck && p_ok && fin(rho_raw) && rho_raw >= 1e-10) return ck[k];
+    return material_sound_speed(M, k, clamp_min(rho_raw), p_arg);
+}
+
 // MixtureEOS::mixture_sound_speed, src/dim/eos.hpp:195-221
 template<int NM>
 DHD double mixture_sound_speed(const Mats& M, double rho_total, double p, const double* alpha,
-                               const double* rho)
+                               const double* rho, const double* ck = nullptr)
 {
     rho_total = clamp_min(rho_total);
+    const bool p_ok = fin(p) && p >= 1e-10;
     p = clamp_min(p);
     double beta_mix = 0.0;
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
         const double rho_k = clamp_min(rho[k]);
-        const double c = material_sound_speed(M, k, rho_k, p);
+        const double c = material_speed_or(M, k, rho[k], p, p_ok, ck);
         beta_mix += dmax(finite_or(alpha[k]), 0.0) / safe_denom(rho_k * c * c, 1e-14);
     }
     return sqrt(1.0 / (rho_total * safe_denom(beta_mix, 1e-14)));
 }
 
 // MixtureEOS::generic_mixture_sound_speed, src/dim/eos.hpp:223-275
+// ck: the material sound speeds of the same primitive (rhs_sound_speeds),
+// reused where their arguments agree (material_speed_or), or nullptr.
 template<int NM>
-DHD double sound_speed_generic(const Mats& M, double rho_total, double p, MixVec<NM> x)
+DHD double sound_speed_generic(const Mats& M, double rho_total, double p, MixVec<NM> x,
+                               const double* ck = nullptr)
 {
     const double* alpha = x.alpha;
     const double* rho = x.rho;
     DIMGPU_OPCOUNT(kOpSound);
-    if (M.lambda_model == 0) return mixture_sound_speed<NM>(M, rho_total, p, alpha, rho);
+    if (M.lambda_model == 0) return mixture_sound_speed<NM>(M, rho_total, p, alpha, rho, ck);
+    const bool p_ok = fin(p) && p >= 1e-10;
     double sound_speed[NM], xi[NM];
     double xi_mix = 0.0, inverse_sound_sum = 0.0;
 #pragma unroll
     for (int k = 0; k < NM; ++k) {
         const double alpha_k = dmax(finite_or(alpha[k]), 0.0);
         const double rho_k = clamp_min(rho[k]);
-        sound_speed[k] = material_sound_speed(M, k, rho_k, p);
+        sound_speed[k] = material_speed_or(M, k, rho[k], p, p_ok, ck);
         xi[k] = rho_k * material_energy_pressure_derivative(M, k, rho_k, p);
         xi_mix += alpha_k * xi[k];
         inverse_sound_sum += alpha_k / safe_denom(sound_speed[k], 1e-14);

@@ -373,6 +373,25 @@ int sound_impl(const dimgpu_desc* d, int n, const double* in, double* c)
     return 0;
 }
 
+// The generic sound speed with and without stage A's material speeds ck
+// (rhs_sound_speeds of a primitive with the record's rho_k and p).
+template<int NM, int D>
+int sound_ck_impl(const dimgpu_desc* d, int n, const double* in, double* with_ck, double* without_ck)
+{
+    const Mats M = mats_of(d);
+    for (int i = 0; i < n; ++i) {
+        const double* r = in + (size_t)i * (2 + 2 * NM);
+        Prim<NM, D> P{};
+        P.p = r[1];
+        for (int k = 0; k < NM; ++k) P.rho[k] = r[2 + NM + k];
+        double ck[NM];
+        rhs_sound_speeds<NM, D>(M, P, ck);
+        with_ck[i] = sound_speed_generic<NM>(M, r[0], r[1], mix_of<NM>(r + 2, r + 2 + NM), ck);
+        without_ck[i] = sound_speed_generic<NM>(M, r[0], r[1], mix_of<NM>(r + 2, r + 2 + NM), nullptr);
+    }
+    return 0;
+}
+
 template<int NM, int D>
 int rhs_impl(const dimgpu_desc* d, int n, const double* P, double* rhs)
 {
@@ -432,6 +451,10 @@ int host_repair_state(const dimgpu_desc* d, int n, double* U) { DISPATCH(d, repa
 int host_mixture_pressure(const dimgpu_desc* d, int n, const double* in, double* p) { DISPATCH(d, pressure_impl, d, n, in, p); }
 int host_mixture_sound_speed(const dimgpu_desc* d, int n, const double* in, double* c) { DISPATCH(d, sound_impl, d, n, in, c); }
 int host_alpha_rhs(const dimgpu_desc* d, int n, const double* P, double* rhs) { DISPATCH(d, rhs_impl, d, n, P, rhs); }
+int host_sound_ck(const dimgpu_desc* d, int n, const double* in, double* with_ck, double* without_ck)
+{
+    DISPATCH(d, sound_ck_impl, d, n, in, with_ck, without_ck);
+}
 int host_hllc(const dimgpu_desc* d, int n, int dir, const double* UL, const double* UR, double* out)
 {
     DISPATCH(d, hllc_impl, d, n, dir, UL, UR, out);

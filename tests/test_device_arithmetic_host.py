@@ -175,3 +175,38 @@ def test_fastdiv_divides_every_index_exactly(host):
         xx = x.astype(np.uint64)
         assert np.array_equal(q.astype(np.uint64), xx // d), d
         assert np.array_equal(r.astype(np.uint64), xx % d), d
+
+
+@pytest.mark.parametrize("lam", (0, 1, 2))
+@pytest.mark.parametrize("mi", range(len(MATS)))
+def test_sound_speed_reuses_stage_a_speeds_bit_for_bit(host, mi, lam):
+    """The fused CFL passes stage A's alpha-RHS material sound speeds into the
+    mixture sound speed, which takes them where both evaluate
+    material_sound_speed on the same arguments: the result must equal the
+    one that evaluates every speed itself, bit for bit, for every λ-model,
+    including densities and pressures at and around the two clamps' floors
+    (1e-12, 1e-10), zero, negative and non-finite."""
+    mats = MATS[mi]
+    nm = len(mats)
+    d = abi.make_desc(dim=1, N=(8,), dx=(1.0,), materials=mats, lambda_model=lam)
+    rng = np.random.default_rng(100 + 10 * mi + lam)
+    n = 20000
+    edge = np.array([0.0, -1.0, 1e-13, 1e-12, 5e-11, 1e-10, np.nextafter(1e-10, 0), np.nextafter(1e-10, 1),
+                     2e-10, np.inf, np.nan, 1.0])
+    rec = np.empty((n, 2 + 2 * nm))
+    rec[:, 0] = np.exp(rng.uniform(np.log(1e-3), np.log(2e3), n))
+    rec[:, 1] = np.exp(rng.uniform(np.log(1e3), np.log(1e10), n))
+    a = rng.dirichlet(np.ones(nm), n)
+    rec[:, 2:2 + nm] = a
+    rec[:, 2 + nm:] = np.exp(rng.uniform(np.log(1e-2), np.log(2e3), (n, nm)))
+    pick = rng.random(n) < 0.3
+    rec[pick, 1] = rng.choice(edge, pick.sum())
+    for k in range(nm):
+        pick = rng.random(n) < 0.2
+        rec[pick, 2 + nm + k] = rng.choice(edge, pick.sum())
+    rec = np.ascontiguousarray(rec)
+    w = np.empty(n)
+    wo = np.empty(n)
+    f = host.lib.host_sound_ck
+    assert f(C.byref(d), C.c_int(n), dptr(rec), dptr(w), dptr(wo)) == 0
+    assert bitwise_equal(w, wo)
