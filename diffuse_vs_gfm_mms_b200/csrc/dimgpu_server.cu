@@ -241,7 +241,8 @@ std::string session_message(const dimgpu_session* sess)
 // Admission (lock held): first come first served within the solo lanes and
 // within each batch group; a lane kind or group whose head cannot be taken
 // now (no free lane, no room, or its batch lane is mid-quantum) takes
-// nothing more this round, so its later requests cannot overtake it.
+// nothing more in this admission pass, so its later requests cannot
+// overtake it.
 void admit(dimgpu_server* s)
 {
     std::vector<char> blocked(s->groups.size() + 16, 0);
