@@ -24,7 +24,9 @@ struct dimgpu_batch;
 
 // Per-kernel resident blocks per SM of stages A, B's cell update, D and E.
 // Measured on a B200: A and B's update at 4 (64 registers) 1.9 % (c1) and
-// 2.6 % (c2) less time per step than at 3; D and E at 4 slower.
+// 2.6 % (c2) less time per step than at 3 (on the build with FastDiv item
+// indices: c1 0.575 against 0.587 ms, c2 216.2 against 222.8); D and E at
+// 4 slower.
 #ifndef DIMGPU_A_MINB
 #define DIMGPU_A_MINB 4
 #endif
@@ -40,7 +42,8 @@ struct dimgpu_batch;
 
 // Resident blocks per SM of the per-face-state kernels (staged_bf, staged_c),
 // whose threads carry one face state each: 64 registers.  Measured on a
-// B200: 3.5 % less time per step on c2 (512^3) than at 3 blocks, 0.3 % on c1.
+// B200: 3.5 % less time per step on c2 (512^3) than at 3 blocks, 0.3 % on c1;
+// at 5 (51 registers) c1 0.590 against 0.575 ms, c2 222.5 against 216.2.
 #ifndef DIMGPU_FACE_MINB
 #define DIMGPU_FACE_MINB 4
 #endif
