@@ -228,6 +228,32 @@ def test_multi_chunk_3d_lines_match_oracle(port):
         assert np.all(np.isfinite(cur))
 
 
+@pytest.mark.parametrize("precision", [abi.PRECISION_FP64, abi.PRECISION_MIXED])
+def test_multi_chunk_step_matches_separate_calls(precision):
+    """A step on a grid of several scratch chunks (256 x 256 x 260: the CFL
+    runs as its own pass, every sweep as two chunks of whole lines) must
+    equal, bit for bit, the same step taken as separate calls (CFL, then
+    each sweep with its boundary fill), whose sweeps match the oracle line
+    by line (test_multi_chunk_3d_lines_match_oracle); FP64 and mixed."""
+    N = (256, 256, 260)
+    d, U = W.bubble_cloud_3d(N=N, nbubbles=64)
+    d.precision = precision
+    with Session(d, U) as s:
+        dts = s.steps(2, 0.6, 1e300)
+        out = s.download()
+    ref_dts = []
+    with Session(d, U) as s:
+        for _ in range(2):
+            dt = s.compute_dt_cfl(0.6, 1e300)
+            ref_dts.append(dt)
+            for direction in range(3):
+                s.sweep_direction(direction, dt)
+                s.apply_boundary_conditions()
+        ref = s.download()
+    assert bitwise_equal(np.asarray(dts), np.asarray(ref_dts))
+    assert ndiff(out, ref) == 0
+
+
 def test_repeatable():
     d, U = W.shock_bubble_2d(N=(256, 128))
     res = []
